@@ -1,0 +1,446 @@
+#!/usr/bin/env python
+"""Benchmark of the batched FFT engine on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Workloads (synthetic, seeded; shapes from the reference benchmark configs):
+  rfft12      RFFT<float> order 12 (N = 4096), 8192 Hann-windowed frames of
+              3 sinusoids + N(0, 0.1^2) noise; one step = forward to AoS,
+              forward to split SoA and forward_sqr_mag over the whole batch
+              (plain FP32 CUDA-core form).
+
+Metric: algorithmic HBM bytes (one read of each input, one write of each
+output; twiddles excluded) per second, in GB/s; roofline = the measured HBM
+copy bandwidth in MEASURED_PEAKS.json. Inputs: two rotating buffer sets, each
+step touching > 2x the 126 MB L2, so no step starts with its data in L2.
+
+--impl reference times the reference's own CPU code (zldsp::fft compiled
+against the project's Highway-API shim, oracle/_ref) on all host cores, on a
+bounded sample of the same workload, and prints the same metric.
+
+Multi-GPU: replicas only (every transform is independent): each rank runs
+the whole workload on its own GPU; value = bytes of all ranks / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Batched FFT HBM GB/s (% of roofline), TC-split vs plain FP32 at equal error"
+
+
+# ------------------------------------------------------------------ helpers
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if d.get("hbm_gbs"):
+            return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key: str):
+    """DRAM bytes per launch from the committed ncu summary (profiles/ncu_traffic.json)."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(kernel_key)
+    return None if v is None else float(v.get("dram_bytes_per_launch")) if isinstance(v, dict) else float(v)
+
+
+class ClockSampler:
+    """Samples SM clock, power and throttle reasons through NVML in a thread."""
+
+    REASONS = {
+        "gpu_idle": 0x1, "applications_clocks_setting": 0x2, "sw_power_cap": 0x4, "hw_slowdown": 0x8,
+        "sync_boost": 0x10, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+        "hw_power_brake_slowdown": 0x80, "display_clock_setting": 0x100,
+    }
+
+    def __init__(self, device_index: int, period_s: float = 0.002):
+        self.idx = device_index
+        self.period = period_s
+        self.samples = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.ok = False
+
+    def _sample(self):
+        nv = self.nv
+        sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+        try:
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        except Exception:
+            reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+        try:
+            pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+        except Exception:
+            pw = None
+        self.samples.append((sm, reasons, pw))
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def start(self):
+        if self.ok:
+            self._sample()
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+
+    def stop(self):
+        if self.ok and self._t:
+            self._stop.set()
+            self._t.join()
+            self._sample()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"], "samples": 0}
+        mhz = [s[0] for s in self.samples]
+        mask = 0
+        for s in self.samples:
+            mask |= int(s[1])
+        reasons = [k for k, v in self.REASONS.items() if mask & v and k != "gpu_idle"]
+        pw = [s[2] for s in self.samples if s[2] is not None]
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples), "power_w_max": max(pw) if pw else None}
+
+
+# ------------------------------------------------------------------ workloads
+def hann_frames(b, n, seed):
+    """3 sinusoids (f ~ U(0, 0.5) cycles/sample, A ~ U[0.1, 1], phase ~ U[0, 2pi))
+    + N(0, 0.1^2) noise, times a periodic Hann window."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(n, dtype=np.float64)
+    w = 0.5 - 0.5 * np.cos(2 * np.pi * t / n)
+    out = np.empty((b, n), np.float32)
+    chunk = 1024
+    for s in range(0, b, chunk):
+        e = min(b, s + chunk)
+        m = e - s
+        f = rng.uniform(0, 0.5, (m, 3, 1))
+        a = rng.uniform(0.1, 1, (m, 3, 1))
+        ph = rng.uniform(0, 2 * np.pi, (m, 3, 1))
+        sig = (a * np.sin(2 * np.pi * f * t + ph)).sum(1) + rng.normal(0, 0.1, (m, n))
+        out[s:e] = (sig * w).astype(np.float32)
+    return out
+
+
+class Rfft12:
+    name = "rfft12"
+    desc = "RFFT<float> order 12 (N=4096) x 8192 frames: forward AoS + forward SoA + forward_sqr_mag"
+    order, n, batch = 12, 4096, 8192
+    dtype = "f32"
+
+    def __init__(self):
+        n, nb, b = self.n, self.n // 2 + 1, self.batch
+        self.nb = nb
+        self.op_bytes = {  # algorithmic bytes of one op over the batch
+            "r2c_fwd_aos": b * (4 * n + 8 * nb),
+            "r2c_fwd_soa": b * (4 * n + 8 * nb),
+            "r2c_sqr_mag": b * (4 * n + 4 * nb),
+        }
+        self.bytes_per_step = sum(self.op_bytes.values())
+        self.dominant = "r2c_fwd_aos"
+
+    # ---- GPU (ours)
+    def setup(self, device):
+        import torch
+        import zldsp_fft_b200 as Z
+        self.Z = Z
+        self.plan = Z.Plan(Z.R2C, self.order, np.float32, device=device)
+        host = hann_frames(self.batch, self.n, 1002)
+        self.host_in = host
+        b, n, nb = self.batch, self.n, self.nb
+        self.sets = []
+        for _ in range(2):  # rotating sets: each step reads/writes > 2x L2
+            d = {
+                "in": torch.from_numpy(host).to(device),
+                "aos": torch.empty((b, nb, 2), dtype=torch.float32, device=device),
+                "re": torch.empty((b, nb), dtype=torch.float32, device=device),
+                "im": torch.empty((b, nb), dtype=torch.float32, device=device),
+                "sqr": torch.empty((b, nb), dtype=torch.float32, device=device),
+            }
+            self.sets.append(d)
+        torch.cuda.synchronize(device)
+
+    def ops(self, step):
+        """[(op_name, launch_fn)] for one step on rotating set step % 2."""
+        Z, p, d = self.Z, self.plan, self.sets[step % 2]
+        b = self.batch
+
+        def fwd_aos(st):
+            p.exec_device(Z.FORWARD, Z.AOS, Z.AOS, d["in"].data_ptr(), None, d["aos"].data_ptr(), None, b, stream=st)
+
+        def fwd_soa(st):
+            p.exec_device(Z.FORWARD, Z.AOS, Z.SOA, d["in"].data_ptr(), None, d["re"].data_ptr(), d["im"].data_ptr(),
+                          b, stream=st)
+
+        def sqr(st):
+            p.exec_device(Z.FORWARD_SQR_MAG, Z.AOS, Z.AOS, d["in"].data_ptr(), None, d["sqr"].data_ptr(), None, b,
+                          stream=st)
+
+        return [("r2c_fwd_aos", fwd_aos), ("r2c_fwd_soa", fwd_soa), ("r2c_sqr_mag", sqr)]
+
+    def take_launches(self):
+        return self.plan.take_launch_count()
+
+    # ---- end to end through the host API (pinned host buffers)
+    def setup_e2e(self):
+        import torch
+        b, n, nb = self.batch, self.n, self.nb
+        self.h_in = torch.from_numpy(self.host_in).pin_memory()
+        self.h_aos = torch.empty((b, nb, 2), dtype=torch.float32).pin_memory()
+        self.h_re = torch.empty((b, nb), dtype=torch.float32).pin_memory()
+        self.h_im = torch.empty((b, nb), dtype=torch.float32).pin_memory()
+        self.h_sqr = torch.empty((b, nb), dtype=torch.float32).pin_memory()
+        self.e2e_h2d = 3 * self.h_in.numel() * 4
+        self.e2e_d2h = (self.h_aos.numel() + self.h_re.numel() + self.h_im.numel() + self.h_sqr.numel()) * 4
+
+    def e2e_step(self):
+        Z, p, b = self.Z, self.plan, self.batch
+        p.exec_host(Z.FORWARD, Z.AOS, Z.AOS, self.h_in.data_ptr(), None, self.h_aos.data_ptr(), None, b)
+        p.exec_host(Z.FORWARD, Z.AOS, Z.SOA, self.h_in.data_ptr(), None, self.h_re.data_ptr(), self.h_im.data_ptr(), b)
+        p.exec_host(Z.FORWARD_SQR_MAG, Z.AOS, Z.AOS, self.h_in.data_ptr(), None, self.h_sqr.data_ptr(), None, b)
+
+    # ---- CPU: the reference's own code (or the oracle restatement)
+    def cpu_run(self, frames, threads, kind):
+        from oracle import oracle as O
+        x = self.host_in[:frames]
+        frames = x.shape[0]
+        if kind == "reference":
+            plan = O.RefPlan("r2c", self.order, "f32", threads)
+            outs = (np.empty((frames, self.nb), np.complex64),
+                    (np.empty((frames, self.nb), np.float32), np.empty((frames, self.nb), np.float32)),
+                    np.empty((frames, self.nb), np.float32))
+            t0 = time.perf_counter()
+            plan.rfft_forward(x, O.AOS, out=outs[0])
+            plan.rfft_forward(x, O.SOA, out=outs[1])
+            plan.rfft_forward(x, sqr_mag=True, out=outs[2])
+            dt = time.perf_counter() - t0
+            plan.close()
+        else:
+            t0 = time.perf_counter()
+            O.rfft_forward_port(x)
+            O.rfft_forward_port(x)
+            O.rfft_forward_port(x, sqr_mag=True)
+            dt = time.perf_counter() - t0
+        return self.bytes_per_step * frames / self.batch, dt
+
+
+WORKLOADS = {"rfft12": Rfft12}
+
+
+# ------------------------------------------------------------------ CPU baseline
+def cpu_baseline(wl, target_s=3.0, threads=None, kind=None):
+    from oracle import oracle as O
+    if kind is None:
+        kind = "reference" if O.ref_available() else "port"
+    threads = threads or (os.cpu_count() or 1) if kind == "reference" else 1
+    frames = 64
+    avail = wl.host_in.shape[0]
+    nbytes, dt = wl.cpu_run(frames, threads, kind)
+    while dt < target_s / 4 and frames < avail:
+        frames = min(avail, frames * 4)
+        nbytes, dt = wl.cpu_run(frames, threads, kind)
+    runs = [(nbytes, dt)]
+    for _ in range(2):
+        runs.append(wl.cpu_run(frames, threads, kind))
+    gbs = statistics.median(b / t / 1e9 for b, t in runs)
+    return {
+        "value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+        "sample": f"{frames} of {wl.batch} frames, same ops as one step, median of 3",
+    }
+
+
+# ------------------------------------------------------------------ arms
+def run_reference_arm(args, wl_cls):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = wl_cls()
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    threads = os.cpu_count() or 1
+    wl.host_in = hann_frames(min(wl.batch, 2048), wl.n, 1002) if hasattr(wl, "n") else None
+    # each step: a bounded sample of the workload on all host cores
+    frames = 64
+    _, dt = wl.cpu_run(frames, threads, kind)
+    while dt < 0.25 and frames < wl.host_in.shape[0]:
+        frames = min(wl.host_in.shape[0], frames * 2)
+        _, dt = wl.cpu_run(frames, threads, kind)
+    for _ in range(args.warmup):
+        wl.cpu_run(frames, threads, kind)
+    tot_b, tot_t = 0.0, 0.0
+    for _ in range(args.steps):
+        b, t = wl.cpu_run(frames, threads, kind)
+        tot_b += b
+        tot_t += t
+    v = tot_b / tot_t / 1e9
+    line = {
+        "metric": METRIC, "value": round(v, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * tot_t / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic",
+        "config": {"workload": wl.desc, "sample_frames_per_step": frames},
+        "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+                         "sample": f"{frames} of {wl.batch} frames per step, same ops"},
+        "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, wl_cls):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    device = torch.cuda.current_device()
+    wl = wl_cls()
+    wl.setup(device)
+    stream = torch.cuda.current_stream()
+    st = stream.cuda_stream
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for w in range(args.warmup):
+        for _, fn in wl.ops(w):
+            fn(st)
+    torch.cuda.synchronize()
+    wl.take_launches()
+
+    names = [name for name, _ in wl.ops(0)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)] for _ in range(args.steps)]
+    clocks = ClockSampler(device)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for s in range(args.steps):
+        ops = wl.ops(s)
+        ev[s][0].record(stream)
+        for i, (_, fn) in enumerate(ops):
+            fn(st)
+            ev[s][i + 1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clocks.stop()
+    barrier()
+    launches = wl.take_launches()
+    elapsed_ms = t_start.elapsed_time(t_end)
+    per_op_ms = {name: statistics.mean(ev[s][i].elapsed_time(ev[s][i + 1]) for s in range(args.steps))
+                 for i, name in enumerate(names)}
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    total_bytes = wl.bytes_per_step * args.steps * world
+    value = total_bytes / (elapsed_ms / 1e3) / 1e9
+
+    # end to end through the host API, pinned host buffers, copies inside the region
+    wl.setup_e2e()
+    e2e_steps = max(3, min(args.steps, 10))
+    wl.e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        wl.e2e_step()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = wl.bytes_per_step * e2e_steps * world / e2e_s / 1e9
+    wl.take_launches()
+
+    peak, peak_kind = measured_hbm_peak()
+    dom = wl.dominant
+    achieved = wl.op_bytes[dom] / (per_op_ms[dom] / 1e3) / 1e9
+    traffic = ncu_traffic(dom)
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic",
+        "config": {"workload": wl.desc, "form": "plain FP32 (reference's Stockham radix-4/8 DIT, CUDA cores)",
+                   "l2": "rotating input/output sets, each step > 2x L2 (no L2 flush needed)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "kernel": dom, "algorithmic_bytes_per_launch": wl.op_bytes[dom],
+                     "traffic": traffic},
+        "per_op_gbs": {k: round(wl.op_bytes[k] / (v / 1e3) / 1e9, 1) for k, v in per_op_ms.items()},
+        "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": wl.e2e_h2d,
+                "d2h_bytes_per_step": wl.e2e_d2h, "api": "zlfft_exec_host_batched, pinned host buffers"},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        if world == 1 and not args.no_cpu:
+            try:
+                line["cpu_baseline"] = cpu_baseline(wl)
+            except Exception as e:  # the baseline is reported, never required
+                line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rfft12")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    wl_cls = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference_arm(args, wl_cls)
+    return run_ours(args, wl_cls)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

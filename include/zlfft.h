@@ -1,0 +1,141 @@
+/* libzlfft_cuda — C ABI of the B200 FFT engine that stands in for
+ * zldsp::fft::CFFT<F> and zldsp::fft::RFFT<F> (ZL-Audio/zldsp_fft).
+ *
+ * The reference is a header-only C++ library; its "binding surface" is the
+ * two class templates. Every entry point below names the reference member it
+ * replaces (file:line within the reference project). The C++ drop-in headers
+ * in include/zldsp_fft_cuda/ implement those classes over this ABI.
+ *
+ * Conventions (identical to the reference):
+ *   forward   X[k] = sum_n x[n] exp(-2 pi i k n / N)
+ *   backward  unnormalised inverse: CFFT backward(forward(x)) = N * x,
+ *             RFFT backward(forward(x)) = (N/2) * x
+ *   RFFT forward writes N/2+1 bins (DC and Nyquist with zero imaginary part);
+ *   forward_sqr_mag writes the N/2+1 values re^2 + im^2.
+ *
+ * All functions return ZLFFT_OK (0) or a negative status; the message of the
+ * calling thread's last failure is returned by zlfft_last_error().
+ */
+#ifndef ZLFFT_H_
+#define ZLFFT_H_
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define ZLFFT_API __attribute__((visibility("default")))
+#else
+#define ZLFFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct zlfft_plan_s* zlfft_plan;
+
+/* status codes */
+#define ZLFFT_OK 0
+#define ZLFFT_ERR_INVALID_ARG (-1)
+#define ZLFFT_ERR_UNSUPPORTED (-2)
+#define ZLFFT_ERR_ALIGNMENT (-3)
+#define ZLFFT_ERR_CUDA (-4)
+#define ZLFFT_ERR_ALLOC (-5)
+#define ZLFFT_ERR_DEVICE_TIMEOUT (-6)
+
+/* transform kind */
+#define ZLFFT_C2C 0 /* CFFT<F> */
+#define ZLFFT_R2C 1 /* RFFT<F> */
+
+/* precision */
+#define ZLFFT_F32 0
+#define ZLFFT_F64 1
+
+/* complex layout: AoS = interleaved std::complex<F>[], SoA = split {F* re, F* im} */
+#define ZLFFT_AOS 0
+#define ZLFFT_SOA 1
+
+/* operation */
+#define ZLFFT_FORWARD 0
+#define ZLFFT_BACKWARD 1
+#define ZLFFT_FORWARD_SQR_MAG 2 /* RFFT only */
+
+/* computation form */
+#define ZLFFT_MODE_PLAIN 0   /* reference's Stockham radix-4/8 DIT on CUDA cores */
+#define ZLFFT_MODE_TC_FP16 1 /* radix-16 sub-DFTs on tensor cores, split hi/lo FP16 */
+#define ZLFFT_MODE_TC_BF16 2 /* split 3-way BF16 */
+#define ZLFFT_MODE_TC_TF32 3 /* 3xTF32 */
+
+/* Create a plan for one transform size.
+ * Replaces the constructors CFFT<F>::CFFT(size_t order)
+ * (src/zldsp_fft_cfft.hpp:19-23) and RFFT<F>::RFFT(size_t order)
+ * (src/zldsp_fft_rfft.hpp:24-53). order is log2 of the transform length N
+ * (RFFT: real length). Twiddle tables are generated on the device in FP64 and
+ * rounded to the plan's precision. device < 0 means the current device. */
+ZLFFT_API int zlfft_plan_create(zlfft_plan* plan, int kind, int precision, size_t order, int mode, int device);
+
+/* Release a plan and every buffer it owns. Replaces the reference objects'
+ * destructors (members freed by hwy::AlignedFreeUniquePtr,
+ * src/common/zldsp_fft_common_init.hpp:28-42). */
+ZLFFT_API int zlfft_plan_destroy(zlfft_plan plan);
+
+/* N = 2^order. Replaces CFFT::get_size (src/zldsp_fft_cfft.hpp:25-27) and
+ * RFFT::get_size (src/zldsp_fft_rfft.hpp:55-57). */
+ZLFFT_API int zlfft_plan_get_size(zlfft_plan plan, size_t* size);
+
+/* Replaces CFFT::get_order (src/zldsp_fft_cfft.hpp:29-31) and
+ * RFFT::get_order (src/zldsp_fft_rfft.hpp:59-61). */
+ZLFFT_API int zlfft_plan_get_order(zlfft_plan plan, size_t* order);
+
+/* One transform on HOST buffers, synchronous (the output is valid on return),
+ * exactly as the reference's member functions behave:
+ *   CFFT forward/backward, 8 overloads (src/zldsp_fft_cfft.hpp:38-103):
+ *     op = FORWARD|BACKWARD, in_layout/out_layout = AOS|SOA;
+ *     AoS uses in0/out0 (complex array), SoA uses (in0 = re, in1 = im).
+ *   RFFT::forward(F*, C*) / forward(F*, std::array<F*,2>) (src/zldsp_fft_rfft.hpp:68-80):
+ *     op = FORWARD, in0 = real input, out_layout selects AoS/SoA bins.
+ *   RFFT::backward(C*, F*) / backward(std::array<F*,2>, F*) (src/zldsp_fft_rfft.hpp:86-98):
+ *     op = BACKWARD, in_layout selects AoS/SoA bins, out0 = real output.
+ *   RFFT::forward_sqr_mag(F*, F*) (src/zldsp_fft_rfft.hpp:104-109):
+ *     op = FORWARD_SQR_MAG, in0 = real input, out0 = N/2+1 reals.
+ * Inputs are not modified. CFFT may run in place (in == out, same layout). */
+ZLFFT_API int zlfft_exec_host(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0, const void* in1,
+                    void* out0, void* out1);
+
+/* As zlfft_exec_host for `batch` transforms laid out back to back (stride =
+ * the transform's own element count). No reference counterpart: a batched
+ * form of the calls above, staged through the plan's pinned buffers. */
+ZLFFT_API int zlfft_exec_host_batched(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0,
+                            const void* in1, void* out0, void* out1, size_t batch);
+
+/* Batched transforms on DEVICE buffers, asynchronous on `stream`
+ * (a cudaStream_t; NULL = legacy default stream). No reference counterpart:
+ * the device-pointer batched entry point that sits beside the reference's
+ * calls above. Transform b reads element e at in + b*in_stride + e and writes
+ * out + b*out_stride + e, strides counted in elements of the buffer's own
+ * type (complex for complex buffers, real for real buffers; 0 = dense).
+ * Pointers must be aligned to the element type (8 B f32 complex, 16 B f64
+ * complex); RFFT real buffers need an even stride. */
+ZLFFT_API int zlfft_exec_device(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0, const void* in1,
+                      void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, void* stream);
+
+/* Number of CUDA kernels launched by this plan on the calling thread since
+ * the last call (diagnostics for benchmarks). */
+ZLFFT_API int zlfft_plan_take_launch_count(zlfft_plan plan, size_t* launches);
+
+/* Copy the plan's unified twiddle table T[t] = exp(-2 pi i t / M), t < 3M/4,
+ * to host memory (M = CFFT length; RFFT plans: N/2), as interleaved
+ * re/im pairs of the plan precision. `count` receives 3M/4. Diagnostics: lets
+ * a caller compare the device-generated table with the reference's. */
+ZLFFT_API int zlfft_plan_copy_twiddles(zlfft_plan plan, void* host_out, size_t capacity_elems, size_t* count);
+
+/* Message of the calling thread's last failure ("" if none). */
+ZLFFT_API const char* zlfft_last_error(void);
+
+/* Library version string. */
+ZLFFT_API const char* zlfft_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZLFFT_H_ */

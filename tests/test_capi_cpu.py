@@ -1,0 +1,61 @@
+"""C ABI checks that need no GPU: the library loads, exports every symbol
+include/zlfft.h declares, and rejects invalid arguments before touching CUDA
+(the reference has no defined behaviour for these; the ABI reports them)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import zldsp_fft_b200 as Z
+from zldsp_fft_b200 import _capi as C
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "zlfft.h")).read()
+    return sorted(set(re.findall(r"ZLFFT_API\s+(?:const\s+)?\w+\*?\s+\**(zlfft_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.lib()
+    declared = _declared()
+    assert declared, "no declarations parsed"
+    assert sorted(C.EXPORTS) == declared
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert "sm_100a" in C.version()
+
+
+def test_invalid_arguments_rejected_without_cuda():
+    lib = C.lib()
+    h = ctypes.c_void_p()
+    assert lib.zlfft_plan_create(None, 0, 0, 4, 0, -1) == C.ERR_INVALID_ARG
+    assert lib.zlfft_plan_create(ctypes.byref(h), 7, 0, 4, 0, -1) == C.ERR_INVALID_ARG
+    assert lib.zlfft_plan_create(ctypes.byref(h), 0, 5, 4, 0, -1) == C.ERR_INVALID_ARG
+    assert lib.zlfft_plan_create(ctypes.byref(h), 0, 0, 31, 0, -1) == C.ERR_INVALID_ARG
+    # the reference's RFFT(0) underflows (src/zldsp_fft_rfft.hpp:26); the ABI refuses it
+    assert lib.zlfft_plan_create(ctypes.byref(h), C.R2C, 0, 0, 0, -1) == C.ERR_INVALID_ARG
+    assert "RFFT order" in C.last_error()
+    assert lib.zlfft_exec_device(None, 0, 0, 0, None, None, None, None, 1, 0, 0, None) == C.ERR_INVALID_ARG
+    assert lib.zlfft_plan_destroy(None) == C.OK
+    sz = ctypes.c_size_t()
+    assert lib.zlfft_plan_get_size(None, ctypes.byref(sz)) == C.ERR_INVALID_ARG
+
+
+def test_python_mirror_rejects_bad_buffers():
+    from zldsp_fft_b200.fft import _complex_arg, _real_arg
+    import numpy as np
+    with pytest.raises(ValueError):
+        _complex_arg(np.zeros(4, np.complex128), 8, np.complex64, np.float32, "in", False)
+    with pytest.raises(ValueError):
+        _complex_arg((np.zeros(8, np.float32),), 8, np.complex64, np.float32, "in", False)
+    with pytest.raises(ValueError):
+        _real_arg(np.zeros(3, np.float32), 8, np.float32, "in", False)
+    ro = np.zeros(8, np.float32)
+    ro.flags.writeable = False
+    with pytest.raises(ValueError):
+        _real_arg(ro, 8, np.float32, "out", True)
+    with pytest.raises(TypeError):
+        Z.fft._prec(np.int32)

@@ -1,0 +1,236 @@
+"""GPU parity: the CUDA kernels, called through the C ABI on device buffers,
+against the oracle on the same seeded inputs.
+
+Tolerance (north star): relative L2 <= 4*log2(N)*eps against the FP64 oracle
+(eps = 2^-24 f32, 2^-53 f64). The plain form rebuilds the reference's own
+arithmetic, so in f32 (where the device-generated twiddle table is bit-equal
+to the reference's) the output must also be BIT-IDENTICAL to the oracle's C
+restatement, which is itself bit-identical to the reference's code.
+"""
+import numpy as np
+import pytest
+
+import zldsp_fft_b200 as Z
+from tests import gpu_util as G
+
+pytestmark = pytest.mark.gpu
+
+PRECS = [("f32", np.float32, np.complex64), ("f64", np.float64, np.complex128)]
+TILE_ORDERS = list(range(0, 14))
+
+
+def _cx(rng, b, n, ct):
+    return (rng.uniform(-1, 1, (b, n)) + 1j * rng.uniform(-1, 1, (b, n))).astype(ct)
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+def test_device_twiddles_equal_reference_table(oracle, prec, ft, ct):
+    for order in (2, 4, 7, 10, 13):
+        plan = Z.Plan(Z.C2C, order, ft)
+        T = plan.twiddles()
+        ref = oracle.twiddles(order, prec)
+        if prec == "f32":
+            assert np.array_equal(T, ref), order
+        else:  # the device's double cos/sin vs the host libm's: within a few ulp
+            assert np.abs(T - ref).max() <= 4 * 2.0 ** -53, order
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+@pytest.mark.parametrize("order", TILE_ORDERS)
+def test_cfft_all_layouts(oracle, prec, ft, ct, order):
+    n = 1 << order
+    rng = np.random.default_rng(1000 + order)
+    b = 3 if order < 12 else 2
+    x = _cx(rng, b, n, ct)
+    plan = Z.Plan(Z.C2C, order, ft)
+    tol = oracle.tolerance(order, prec)
+    for forward in (True, False):
+        port = oracle.cfft_port(x, forward)
+        fp64 = oracle.cfft_fp64(x, forward)
+        for il in (Z.AOS, Z.SOA):
+            for ol in (Z.AOS, Z.SOA):
+                y = G.run_c2c(plan, x, forward, il, ol)
+                err = oracle.rel_l2(y, fp64).max()
+                assert err <= tol, (order, forward, il, ol, err)
+                if prec == "f32":
+                    assert np.array_equal(y, port), (order, forward, il, ol)
+                else:
+                    assert oracle.rel_l2(y, port).max() <= tol
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+@pytest.mark.parametrize("order", list(range(1, 15)))
+def test_rfft_forward_sqr_backward(oracle, prec, ft, ct, order):
+    n = 1 << order
+    rng = np.random.default_rng(2000 + order)
+    b = 3
+    x = rng.uniform(-1, 1, (b, n)).astype(ft)
+    plan = Z.Plan(Z.R2C, order, ft)
+    tol = oracle.tolerance(order, prec)
+    port = oracle.rfft_forward_port(x)
+    for ol in (Z.AOS, Z.SOA):
+        X = G.run_r2c(plan, x, ol)
+        assert oracle.rel_l2(X, oracle.rfft_fp64(x)).max() <= tol
+        if prec == "f32":
+            assert np.array_equal(X, port), (order, ol)
+    P = G.run_r2c(plan, x, sqr_mag=True)
+    assert oracle.rel_l2(P, np.abs(oracle.rfft_fp64(x)) ** 2).max() <= 2 * tol
+    if prec == "f32":
+        assert np.array_equal(P, oracle.rfft_forward_port(x, sqr_mag=True)), order
+    Xin = _cx(rng, b, n // 2 + 1, ct)
+    for il in (Z.AOS, Z.SOA):
+        back = G.run_c2r(plan, Xin, il)
+        assert oracle.rel_l2(back, oracle.rfft_backward_fp64(Xin)).max() <= tol
+        if prec == "f32":
+            assert np.array_equal(back, oracle.rfft_backward_port(Xin)), (order, il)
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+def test_golden_reference_outputs(prec, ft, ct):
+    """The reference's own outputs (fixtures) reproduced on the GPU."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", f"reference_{prec}.npz"))
+    for order in range(0, 11):
+        plan = Z.Plan(Z.C2C, order, ft)
+        x = g[f"c2c_{order}_in"]
+        y = G.run_c2c(plan, x, True)
+        yb = G.run_c2c(plan, x, False)
+        if prec == "f32":
+            assert np.array_equal(y, g[f"c2c_{order}_fwd"]) and np.array_equal(yb, g[f"c2c_{order}_bwd"]), order
+    for order in range(1, 12):
+        plan = Z.Plan(Z.R2C, order, ft)
+        x = g[f"r2c_{order}_in"]
+        X = G.run_r2c(plan, x)
+        if prec == "f32":
+            assert np.array_equal(X, g[f"r2c_{order}_fwd"]), order
+            assert np.array_equal(G.run_r2c(plan, x, sqr_mag=True), g[f"r2c_{order}_sqr"]), order
+            assert np.array_equal(G.run_c2r(plan, g[f"r2c_{order}_bins"]), g[f"r2c_{order}_bwd"]), order
+
+
+def test_config1_order10_single_transform(oracle):
+    """CFFT<float> order 10, one transform, AoS: forward then backward, through
+    the reference-shaped host API (zldsp::fft::CFFT::forward/backward)."""
+    rng = np.random.default_rng(1001)
+    n = 1024
+    x = (rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)).astype(np.complex64)
+    cf = Z.CFFT(10)
+    assert cf.get_size() == 1024 and cf.get_order() == 10
+    y = np.zeros_like(x)
+    cf.forward(x, y)
+    back = np.zeros_like(x)
+    cf.backward(y, back)
+    assert np.array_equal(y, oracle.cfft_port(x, True))
+    assert np.array_equal(back, oracle.cfft_port(y, False))
+    assert oracle.rel_l2(y, oracle.cfft_fp64(x)).max() <= oracle.tolerance(10)
+    assert oracle.rel_l2(back, 1024 * x.astype(np.complex128)).max() <= 2 * oracle.tolerance(10)
+    # SoA overloads of the reference: (re, im) pairs
+    re, im = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    cf.forward(x, (re, im))
+    assert np.array_equal(re + 1j * im, y)
+    out = np.zeros_like(x)
+    cf.forward((np.ascontiguousarray(x.real), np.ascontiguousarray(x.imag)), out)
+    assert np.array_equal(out, y)
+
+
+def test_rfft_host_api_overloads(oracle):
+    rng = np.random.default_rng(1002)
+    for order in (1, 2, 5, 12):
+        n = 1 << order
+        x = rng.uniform(-1, 1, n).astype(np.float32)
+        rf = Z.RFFT(order)
+        assert rf.get_size() == n and rf.get_order() == order
+        X = np.zeros(n // 2 + 1, np.complex64)
+        rf.forward(x, X)
+        assert np.array_equal(X, oracle.rfft_forward_port(x))
+        re, im = np.zeros(n // 2 + 1, np.float32), np.zeros(n // 2 + 1, np.float32)
+        rf.forward(x, (re, im))
+        assert np.array_equal(re + 1j * im, X)
+        P = np.zeros(n // 2 + 1, np.float32)
+        rf.forward_sqr_mag(x, P)
+        assert np.array_equal(P, oracle.rfft_forward_port(x, sqr_mag=True))
+        back = np.zeros(n, np.float32)
+        rf.backward(X, back)
+        assert np.array_equal(back, oracle.rfft_backward_port(X))
+        back2 = np.zeros(n, np.float32)
+        rf.backward((re, im), back2)
+        assert np.array_equal(back2, back)
+
+
+def test_config2_rfft_order12_batch8192(oracle):
+    """RFFT<float> order 12 x 8192 Hann-windowed frames (3 sinusoids + noise):
+    full batch on the GPU, a sample of frames checked bit-exactly, every frame
+    checked by size-independent properties."""
+    import torch
+    n, b = 4096, 8192
+    rng = np.random.default_rng(1002)
+    t = np.arange(n)
+    f = rng.uniform(0, 0.5, (b, 3, 1))
+    amp = rng.uniform(0.1, 1, (b, 3, 1))
+    ph = rng.uniform(0, 2 * np.pi, (b, 3, 1))
+    sig = (amp * np.sin(2 * np.pi * f * t + ph)).sum(1) + rng.normal(0, 0.1, (b, n))
+    x = (sig * (0.5 - 0.5 * np.cos(2 * np.pi * t / n))).astype(np.float32)
+    plan = Z.Plan(Z.R2C, 12, np.float32)
+    X = G.run_r2c(plan, x)
+    P = G.run_r2c(plan, x, sqr_mag=True)
+    sample = rng.choice(b, 16, replace=False)
+    assert np.array_equal(X[sample], oracle.rfft_forward_port(x[sample]))
+    assert np.array_equal(P[sample], oracle.rfft_forward_port(x[sample], sqr_mag=True))
+    # every frame: DC/Nyquist real, |X|^2 consistent with sqr_mag, round trip N/2
+    assert np.all(X[:, 0].imag == 0) and np.all(X[:, -1].imag == 0)
+    mag = X.real.astype(np.float64) ** 2 + X.imag.astype(np.float64) ** 2
+    assert oracle.rel_l2(P, mag).max() <= 2 * oracle.tolerance(12)
+    back = G.run_c2r(plan, X)
+    assert oracle.rel_l2(back, (n / 2) * x.astype(np.float64)).max() <= 2 * oracle.tolerance(12)
+    del torch
+
+
+def test_batch_strides_inplace_and_edges(oracle):
+    import torch
+    rng = np.random.default_rng(7)
+    order, n = 9, 512
+    plan = Z.Plan(Z.C2C, order, np.float32)
+    # ragged strides: transforms at stride n + 37 in, n + 5 out
+    b, si, so = 5, n + 37, n + 5
+    buf = (rng.uniform(-1, 1, (b * si)) + 1j * rng.uniform(-1, 1, (b * si))).astype(np.complex64)
+    ti = G.dev(buf)
+    to = torch.zeros((b * so, 2), dtype=torch.float32, device="cuda")
+    plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, ti.data_ptr(), None, to.data_ptr(), None, b, si, so)
+    torch.cuda.synchronize()
+    out = G.host(to)
+    out = out[:, 0] + 1j * out[:, 1]
+    for i in range(b):
+        assert np.array_equal(out[i * so: i * so + n].astype(np.complex64),
+                              oracle.cfft_port(buf[i * si: i * si + n][None, :], True)[0])
+    # in place
+    x = (rng.uniform(-1, 1, (4, n)) + 1j * rng.uniform(-1, 1, (4, n))).astype(np.complex64)
+    t = G.dev(x)
+    plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, t.data_ptr(), None, t.data_ptr(), None, 4)
+    torch.cuda.synchronize()
+    assert np.array_equal(G.host(t), oracle.cfft_port(x, True))
+    # batch 0 is a no-op; misaligned and null pointers are rejected
+    plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, t.data_ptr(), None, t.data_ptr(), None, 0)
+    with pytest.raises(Z.ZlfftError) as e:
+        plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, t.data_ptr() + 4, None, to.data_ptr(), None, 1)
+    assert e.value.code == Z._capi.ERR_ALIGNMENT
+    with pytest.raises(Z.ZlfftError) as e:
+        plan.exec_device(Z.FORWARD, Z.SOA, Z.AOS, t.data_ptr(), None, to.data_ptr(), None, 1)
+    assert e.value.code == Z._capi.ERR_INVALID_ARG
+    with pytest.raises(Z.ZlfftError):
+        plan.exec_device(Z.FORWARD_SQR_MAG, Z.AOS, Z.AOS, t.data_ptr(), None, to.data_ptr(), None, 1)
+    # large batch (grid-stride loop over more tiles than resident CTAs)
+    big = (rng.uniform(-1, 1, (40000, 64)) + 1j * rng.uniform(-1, 1, (40000, 64))).astype(np.complex64)
+    p6 = Z.Plan(Z.C2C, 6, np.float32)
+    y = G.run_c2c(p6, big, True)
+    idx = [0, 1, 12345, 39999]
+    assert np.array_equal(y[idx], oracle.cfft_port(big[idx], True))
+
+
+def test_launch_counter():
+    import torch
+    plan = Z.Plan(Z.C2C, 10, np.float32)
+    plan.take_launch_count()
+    x = torch.zeros((8, 1024, 2), device="cuda")
+    for _ in range(3):
+        plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, x.data_ptr(), None, x.data_ptr(), None, 8)
+    torch.cuda.synchronize()
+    assert plan.take_launch_count() == 3

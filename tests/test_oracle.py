@@ -1,0 +1,145 @@
+"""Pins the oracle before anything is checked against it (CPU only).
+
+1. The C restatement reproduces the reference's golden outputs bit for bit
+   (fixtures made from the reference's own code, tests/golden/make_golden.py).
+2. Where the shim-built reference library is present, the restatement equals
+   it bit for bit on fresh seeded inputs, orders 0..18.
+3. Both agree with an independent FP64 FFT (numpy) within 4*log2(N)*eps.
+4. Analytic known answers: impulse, constant, single tone, round-trip scale,
+   Hermitian symmetry and Parseval.
+"""
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+PRECS = [("f32", np.float32, np.complex64), ("f64", np.float64, np.complex128)]
+
+
+def _golden(prec):
+    return np.load(os.path.join(GOLDEN, f"reference_{prec}.npz"))
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+def test_port_matches_reference_golden_cfft(oracle, prec, ft, ct):
+    g = _golden(prec)
+    for order in range(0, 11):
+        x = g[f"c2c_{order}_in"]
+        assert np.array_equal(oracle.cfft_port(x, True), g[f"c2c_{order}_fwd"]), order
+        assert np.array_equal(oracle.cfft_port(x, False), g[f"c2c_{order}_bwd"]), order
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+def test_port_matches_reference_golden_rfft(oracle, prec, ft, ct):
+    g = _golden(prec)
+    for order in range(1, 12):
+        x = g[f"r2c_{order}_in"]
+        assert np.array_equal(oracle.rfft_forward_port(x), g[f"r2c_{order}_fwd"]), order
+        assert np.array_equal(oracle.rfft_forward_port(x, sqr_mag=True), g[f"r2c_{order}_sqr"]), order
+        assert np.array_equal(oracle.rfft_backward_port(g[f"r2c_{order}_bins"]), g[f"r2c_{order}_bwd"]), order
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
+                                                    "libzlref.so")), reason="shim-built reference not present")
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+def test_port_bitwise_equals_reference_library(oracle, prec, ft, ct):
+    rng = np.random.default_rng(99)
+    _, switch = oracle.ref_switch_order(prec)
+    for order in range(0, 19):
+        n = 1 << order
+        b = 2 if order < 15 else 1
+        x = (rng.uniform(-1, 1, (b, n)) + 1j * rng.uniform(-1, 1, (b, n))).astype(ct)
+        if order < switch:  # the reference's micro-only path (its macro path rounds differently)
+            plan = oracle.RefPlan("c2c", order, prec)
+            for fwd in (True, False):
+                assert np.array_equal(oracle.cfft_port(x, fwd), plan.cfft(x, fwd)), (order, fwd)
+            # every layout pairing of the reference gives the same values
+            re, im = np.ascontiguousarray(x.real), np.ascontiguousarray(x.imag)
+            ref_aos = plan.cfft(x, True)
+            for il, inp in ((oracle.AOS, x), (oracle.SOA, (re, im))):
+                for ol in (oracle.AOS, oracle.SOA):
+                    y = plan.cfft(inp, True, il, ol)
+                    y = y if ol == oracle.AOS else (y[0] + 1j * y[1]).astype(ct)
+                    assert np.array_equal(y, ref_aos), (order, il, ol)
+            plan.close()
+        if order >= 1 and order - 1 < switch:
+            xr = rng.uniform(-1, 1, (b, n)).astype(ft)
+            plan = oracle.RefPlan("r2c", order, prec)
+            X = plan.rfft_forward(xr)
+            assert np.array_equal(oracle.rfft_forward_port(xr), X), order
+            assert np.array_equal(oracle.rfft_forward_port(xr, True), plan.rfft_forward(xr, sqr_mag=True)), order
+            assert np.array_equal(oracle.rfft_backward_port(X), plan.rfft_backward(X)), order
+            plan.close()
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+def test_port_within_fp64_tolerance(oracle, prec, ft, ct):
+    rng = np.random.default_rng(5)
+    for order in range(0, 17):
+        n = 1 << order
+        x = (rng.uniform(-1, 1, (2, n)) + 1j * rng.uniform(-1, 1, (2, n))).astype(ct)
+        tol = oracle.tolerance(order, prec)
+        for fwd in (True, False):
+            err = oracle.rel_l2(oracle.cfft_port(x, fwd), oracle.cfft_fp64(x, fwd)).max()
+            assert err <= tol, (order, fwd, err, tol)
+        if order >= 1:
+            xr = rng.uniform(-1, 1, (2, n)).astype(ft)
+            X = oracle.rfft_forward_port(xr)
+            assert oracle.rel_l2(X, oracle.rfft_fp64(xr)).max() <= tol
+            P = oracle.rfft_forward_port(xr, sqr_mag=True)
+            assert oracle.rel_l2(P, np.abs(oracle.rfft_fp64(xr)) ** 2).max() <= 2 * tol
+            back = oracle.rfft_backward_port(X)
+            assert oracle.rel_l2(back, oracle.rfft_backward_fp64(X)).max() <= tol
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+def test_known_answers(oracle, prec, ft, ct):
+    for order in (0, 1, 2, 3, 4, 5, 8, 11):
+        n = 1 << order
+        # impulse -> constant 1
+        x = np.zeros((1, n), ct)
+        x[0, 0] = 1
+        assert np.array_equal(oracle.cfft_port(x, True), np.ones((1, n), ct))
+        # constant -> N at bin 0
+        y = oracle.cfft_port(np.ones((1, n), ct), True)
+        assert abs(y[0, 0] - n) <= 1e-6 * n and np.abs(y[0, 1:]).max(initial=0) <= 1e-5 * n
+        # single tone at bin k -> N at k
+        k = (3 * n) // 7 if n > 1 else 0
+        t = np.exp(2j * np.pi * ((k * np.arange(n)) % n) / n).astype(ct)[None, :]  # exact phase reduction
+        y = oracle.cfft_port(t, True)
+        expect = np.zeros((1, n), np.complex128)
+        expect[0, k] = n
+        assert oracle.rel_l2(y, expect).max() <= 4 * oracle.tolerance(order, prec) + 1e-15
+        # round trip: backward(forward(x)) = N x
+        rng = np.random.default_rng(order)
+        z = (rng.uniform(-1, 1, (1, n)) + 1j * rng.uniform(-1, 1, (1, n))).astype(ct)
+        rt = oracle.cfft_port(oracle.cfft_port(z, True), False)
+        assert oracle.rel_l2(rt, n * z.astype(np.complex128)).max() <= 2 * oracle.tolerance(order, prec)
+        # Parseval: sum |X|^2 = N sum |x|^2
+        X = oracle.cfft_port(z, True).astype(np.complex128)
+        assert abs(np.sum(np.abs(X) ** 2) - n * np.sum(np.abs(z.astype(np.complex128)) ** 2)) <= \
+            8 * oracle.tolerance(order, prec) * n * np.sum(np.abs(z) ** 2) + 1e-12
+    for order in (1, 2, 3, 6, 9, 12):
+        n = 1 << order
+        rng = np.random.default_rng(order + 100)
+        xr = rng.uniform(-1, 1, (1, n)).astype(ft)
+        X = oracle.rfft_forward_port(xr)
+        assert X[0, 0].imag == 0 and X[0, -1].imag == 0  # DC and Nyquist are real
+        back = oracle.rfft_backward_port(X)  # RFFT round trip scales by N/2
+        assert oracle.rel_l2(back, (n / 2) * xr.astype(np.float64)).max() <= 2 * oracle.tolerance(order, prec)
+        # real input: the N/2+1 bins equal the first half of the complex FFT (Hermitian)
+        full = oracle.cfft_fp64(xr.astype(np.complex128))
+        assert oracle.rel_l2(X, full[:, : n // 2 + 1]).max() <= oracle.tolerance(order, prec)
+
+
+def test_twiddle_table_matches_reference_formula(oracle):
+    # T[t] = (F)cos(-2 pi t / N) etc., computed as the reference does (cos(a*pi) in double)
+    for order in (2, 5, 10, 16):
+        n = 1 << order
+        t = np.arange(3 * n // 4)
+        a = t * (-2.0 / n)
+        for prec, ct in (("f32", np.complex64), ("f64", np.complex128)):
+            T = oracle.twiddles(order, prec)
+            expect = (np.cos(a * np.pi) + 1j * np.sin(a * np.pi)).astype(ct)
+            assert np.array_equal(T, expect)

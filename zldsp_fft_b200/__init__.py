@@ -1,0 +1,18 @@
+"""zldsp_fft_b200 — a B200 (sm_100a) FFT engine that is a drop-in for
+zldsp::fft::CFFT<F> and RFFT<F> (ZL-Audio/zldsp_fft).
+
+Layers:
+  include/zlfft.h                 C ABI (the drop-in boundary)
+  include/zldsp_fft_cuda/*.hpp    C++ drop-in classes over the C ABI
+  zldsp_fft_b200/csrc/*.cu        CUDA kernels + C ABI implementation
+  zldsp_fft_b200/fft.py           Python mirror of the reference's classes
+"""
+from . import _capi
+from ._capi import (AOS, BACKWARD, C2C, F32, F64, FORWARD, FORWARD_SQR_MAG, MODE_PLAIN, MODE_TC_BF16,
+                    MODE_TC_FP16, MODE_TC_TF32, R2C, SOA, ZlfftError)
+from .fft import CFFT, RFFT, Plan
+
+__all__ = [
+    "CFFT", "RFFT", "Plan", "ZlfftError", "AOS", "SOA", "C2C", "R2C", "F32", "F64", "FORWARD", "BACKWARD",
+    "FORWARD_SQR_MAG", "MODE_PLAIN", "MODE_TC_FP16", "MODE_TC_BF16", "MODE_TC_TF32",
+]

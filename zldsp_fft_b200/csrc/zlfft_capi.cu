@@ -1,0 +1,485 @@
+// C ABI of libzlfft_cuda (declared in include/zlfft.h).
+//
+// A plan owns, on its device: the unified twiddle table of its CFFT length
+// (generated here in FP64 and rounded to the plan precision, G1), the RFFT
+// split twiddles, and pinned host staging buffers for the
+// host-pointer calls that mirror zldsp::fft::CFFT/RFFT member functions.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/zlfft.h"
+#include "zlfft_launch.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(ZLFFT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define ZL_CUDA(call)                                  \
+    do {                                               \
+        cudaError_t _e = (call);                       \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+    } while (0)
+
+// ------------------------------------------------------------------ G1: twiddles
+// Generated on the device in FP64 with the reference's own formula, then
+// rounded to F: cospi(a) = cos(a * pi), sinpi(a) = sin(a * pi) with a*pi
+// rounded to double first (src/common/zldsp_fft_common_math.hpp:19-24). This
+// keeps the reference's values where a more accurate sincospi(a) would not:
+// e.g. its cos(pi/2) entry is 6.1e-17, not 0. In FP32 the rounded table is
+// bit-identical to the reference's, which makes the plain form's output
+// bit-identical too.
+__device__ __forceinline__ double ref_cospi(double a) { return cos(__dmul_rn(a, 3.141592653589793)); }
+__device__ __forceinline__ double ref_sinpi(double a) { return sin(__dmul_rn(a, 3.141592653589793)); }
+
+// T[t] = exp(-2*pi*i*t/M) for t < 3M/4, a = -2t/M
+// (src/common/zldsp_fft_common_init.hpp:138-162: per stage the reference
+// evaluates cospi(k * (-2/(4L)) * m), which is exactly a for t = m*k*M/(4L)).
+template <typename F>
+__global__ void twiddle_kernel(zlfft::Cx<F>* tw, int order, long long count) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const double a = (double)t * (-2.0 / (double)(1LL << order));
+    zlfft::Cx<F> w;
+    w.x = (F)ref_cospi(a);
+    w.y = (F)ref_sinpi(a);
+    tw[t] = w;
+}
+
+// RFFT split twiddles k = 0..M/2 for real length Nr = 2M:
+// wc = 0.5*cos(2 pi k / Nr), ws = 0.5*sin(2 pi k / Nr) + 0.5, FP64 then rounded
+// (src/common/zldsp_fft_common_init.hpp:374-381). Index 0 is unused.
+template <typename F>
+__global__ void rfft_twiddle_kernel(F* wc, F* ws, int rfft_order, long long count) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const double a = (double)k * (2.0 / (double)(1LL << rfft_order));
+    wc[k] = (F)__dmul_rn(0.5, ref_cospi(a));
+    ws[k] = (F)__dadd_rn(__dmul_rn(0.5, ref_sinpi(a)), 0.5);
+}
+
+struct TablesHolder {
+    zlfft::TileTable f32{};
+    zlfft::TileTable f64{};
+    TablesHolder() {
+        zlfft::fill_tile_c2c_f32(f32);
+        zlfft::fill_tile_r2c_f32(f32);
+        zlfft::fill_tile_c2c_f64(f64);
+        zlfft::fill_tile_r2c_f64(f64);
+    }
+};
+
+const TablesHolder& tables() {
+    static TablesHolder t;
+    return t;
+}
+
+}  // namespace
+
+struct zlfft_plan_s {
+    int kind = 0;
+    int prec = 0;
+    int order = 0;       // transform order (RFFT: real length)
+    int cfft_order = 0;  // inner complex FFT order
+    int mode = 0;
+    int device = 0;
+    int num_sms = 0;
+    size_t esize = 0;  // bytes of one real
+    void* d_tw = nullptr;
+    size_t tw_count = 0;
+    void* d_rwc = nullptr;
+    void* d_rws = nullptr;
+    // host staging
+    cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;
+    void* h_in = nullptr;
+    void* h_out = nullptr;
+    void* d_in = nullptr;
+    void* d_out = nullptr;
+    size_t stage_in_bytes = 0, stage_out_bytes = 0;
+    size_t launches = 0;
+    std::mutex mu;
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (dev >= 0 && dev != prev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+void release(zlfft_plan p) {
+    if (!p) return;
+    DeviceGuard g(p->device);
+    if (p->d_tw) cudaFree(p->d_tw);
+    if (p->d_rwc) cudaFree(p->d_rwc);
+    if (p->d_rws) cudaFree(p->d_rws);
+    if (p->d_in) cudaFree(p->d_in);
+    if (p->d_out) cudaFree(p->d_out);
+    if (p->h_in) cudaFreeHost(p->h_in);
+    if (p->h_out) cudaFreeHost(p->h_out);
+    if (p->stream) cudaStreamDestroy(p->stream);
+    if (p->stream2) cudaStreamDestroy(p->stream2);
+    delete p;
+}
+
+// Elements (of the buffer's own type) that one transform reads or writes.
+struct Extents {
+    size_t in_elems, out_elems;   // count of complex or real elements
+    bool in_complex, out_complex; // element type
+};
+
+Extents extents(const zlfft_plan_s* p, int op) {
+    const size_t n = size_t{1} << p->order;
+    if (p->kind == ZLFFT_C2C) return {n, n, true, true};
+    const size_t nb = n / 2 + 1;
+    if (op == ZLFFT_FORWARD) return {n, nb, false, true};
+    if (op == ZLFFT_FORWARD_SQR_MAG) return {n, nb, false, false};
+    return {nb, n, true, false};
+}
+
+int validate_op(const zlfft_plan_s* p, int op, int in_layout, int out_layout) {
+    if (op < ZLFFT_FORWARD || op > ZLFFT_FORWARD_SQR_MAG) return fail(ZLFFT_ERR_INVALID_ARG, "invalid op %d", op);
+    if (op == ZLFFT_FORWARD_SQR_MAG && p->kind != ZLFFT_R2C)
+        return fail(ZLFFT_ERR_INVALID_ARG, "forward_sqr_mag is an RFFT operation");
+    if ((in_layout != ZLFFT_AOS && in_layout != ZLFFT_SOA) || (out_layout != ZLFFT_AOS && out_layout != ZLFFT_SOA))
+        return fail(ZLFFT_ERR_INVALID_ARG, "invalid layout");
+    return ZLFFT_OK;
+}
+
+int device_op_code(const zlfft_plan_s* p, int op) {
+    if (p->kind == ZLFFT_C2C) return op == ZLFFT_FORWARD ? zlfft::kC2CFwd : zlfft::kC2CBwd;
+    if (op == ZLFFT_FORWARD) return zlfft::kR2CFwd;
+    if (op == ZLFFT_FORWARD_SQR_MAG) return zlfft::kR2CSqrMag;
+    return zlfft::kC2RBwd;
+}
+
+bool aligned(const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(ptr) % a) == 0; }
+
+int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,
+                     void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, cudaStream_t stream) {
+    int rc = validate_op(p, op, in_layout, out_layout);
+    if (rc) return rc;
+    const Extents ex = extents(p, op);
+    const bool in_soa = ex.in_complex && in_layout == ZLFFT_SOA;
+    const bool out_soa = ex.out_complex && out_layout == ZLFFT_SOA;
+    if (!in0 || (in_soa && !in1)) return fail(ZLFFT_ERR_INVALID_ARG, "null input pointer");
+    if (!out0 || (out_soa && !out1)) return fail(ZLFFT_ERR_INVALID_ARG, "null output pointer");
+    if (in_stride == 0) in_stride = ex.in_elems;
+    if (out_stride == 0) out_stride = ex.out_elems;
+    if (batch > 1 && (in_stride < ex.in_elems || out_stride < ex.out_elems))
+        return fail(ZLFFT_ERR_INVALID_ARG, "stride smaller than one transform");
+    // Alignment: AoS complex buffers are read as 8/16-byte vectors; an RFFT
+    // real input is read as complex pairs, so it needs pair alignment and an
+    // even stride; an RFFT real output is written as pairs likewise.
+    const size_t pair = 2 * p->esize;
+    const bool in_pairs = ex.in_complex ? !in_soa : (op != ZLFFT_BACKWARD);
+    const bool out_pairs = ex.out_complex ? !out_soa : (p->kind == ZLFFT_R2C && op == ZLFFT_BACKWARD);
+    if (in_pairs && !aligned(in0, pair)) return fail(ZLFFT_ERR_ALIGNMENT, "input must be %zu-byte aligned", pair);
+    if (out_pairs && !aligned(out0, pair)) return fail(ZLFFT_ERR_ALIGNMENT, "output must be %zu-byte aligned", pair);
+    if (!aligned(in0, p->esize) || (in1 && !aligned(in1, p->esize)) || !aligned(out0, p->esize) ||
+        (out1 && !aligned(out1, p->esize)))
+        return fail(ZLFFT_ERR_ALIGNMENT, "buffers must be aligned to the element type");
+    if (!ex.in_complex && (in_stride % 2)) return fail(ZLFFT_ERR_INVALID_ARG, "RFFT real input stride must be even");
+    if (p->kind == ZLFFT_R2C && op == ZLFFT_BACKWARD && (out_stride % 2))
+        return fail(ZLFFT_ERR_INVALID_ARG, "RFFT real output stride must be even");
+    if (p->kind == ZLFFT_C2C && in0 == out0 && in_layout != out_layout)
+        return fail(ZLFFT_ERR_INVALID_ARG, "in-place transform needs the same layout on both sides");
+    if (batch == 0) return ZLFFT_OK;
+
+    zlfft::TileArgs a;
+    a.in0 = in0;
+    a.in1 = in_soa ? in1 : nullptr;
+    a.out0 = out0;
+    a.out1 = out_soa ? out1 : nullptr;
+    a.batch = (long long)batch;
+    // Strides in units of the element each kernel indexes: real sides of an
+    // RFFT are indexed as complex pairs, except the squared-magnitude output.
+    a.in_stride = (long long)(ex.in_complex ? in_stride : in_stride / 2);
+    a.out_stride = (long long)((ex.out_complex || op == ZLFFT_FORWARD_SQR_MAG) ? out_stride : out_stride / 2);
+    a.tw = p->d_tw;
+    a.rwc = p->d_rwc;
+    a.rws = p->d_rws;
+
+    const int dop = device_op_code(p, op);
+    const int P = p->cfft_order;
+    zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
+    const zlfft::TileTable& t = p->prec == ZLFFT_F32 ? tables().f32 : tables().f64;
+    if (P > zlfft::kTileMaxP) return fail(ZLFFT_ERR_UNSUPPORTED, "order %d not supported yet", p->order);
+    zlfft::TileLaunchFn fn = t.fn[P][dop][in_layout][out_layout];
+    if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no kernel for this configuration");
+    DeviceGuard g(p->device);
+    cudaError_t e = fn(a, stream, ctx);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return ZLFFT_OK;
+}
+
+int ensure_staging(zlfft_plan_s* p, size_t in_bytes, size_t out_bytes) {
+    if (in_bytes > p->stage_in_bytes) {
+        if (p->h_in) cudaFreeHost(p->h_in);
+        if (p->d_in) cudaFree(p->d_in);
+        p->h_in = p->d_in = nullptr;
+        p->stage_in_bytes = 0;
+        if (cudaMallocHost(&p->h_in, in_bytes) != cudaSuccess || cudaMalloc(&p->d_in, in_bytes) != cudaSuccess)
+            return fail(ZLFFT_ERR_ALLOC, "staging allocation of %zu bytes failed", in_bytes);
+        p->stage_in_bytes = in_bytes;
+    }
+    if (out_bytes > p->stage_out_bytes) {
+        if (p->h_out) cudaFreeHost(p->h_out);
+        if (p->d_out) cudaFree(p->d_out);
+        p->h_out = p->d_out = nullptr;
+        p->stage_out_bytes = 0;
+        if (cudaMallocHost(&p->h_out, out_bytes) != cudaSuccess || cudaMalloc(&p->d_out, out_bytes) != cudaSuccess)
+            return fail(ZLFFT_ERR_ALLOC, "staging allocation of %zu bytes failed", out_bytes);
+        p->stage_out_bytes = out_bytes;
+    }
+    return ZLFFT_OK;
+}
+
+bool is_pinned(const void* ptr) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+// Host-pointer path: H2D copy of the input (directly from the caller's
+// buffer when it is page-locked, else through the plan's pinned staging),
+// the device kernel on the plan's stream, D2H copy back, synchronise.
+// The batch is cut into chunks so that the copies of one chunk overlap the
+// kernel and the opposite-direction copy of its neighbours (two streams).
+int exec_host_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,
+                   void* out0, void* out1, size_t batch) {
+    int rc = validate_op(p, op, in_layout, out_layout);
+    if (rc) return rc;
+    const Extents ex = extents(p, op);
+    const bool in_soa = ex.in_complex && in_layout == ZLFFT_SOA;
+    const bool out_soa = ex.out_complex && out_layout == ZLFFT_SOA;
+    if (!in0 || (in_soa && !in1) || !out0 || (out_soa && !out1))
+        return fail(ZLFFT_ERR_INVALID_ARG, "null buffer pointer");
+    if (batch == 0) return ZLFFT_OK;
+    // bytes of one transform on each side, per part (SoA: per re/im array)
+    const size_t in_part = ex.in_elems * (ex.in_complex && !in_soa ? 2 : 1) * p->esize;
+    const size_t out_part = ex.out_elems * (ex.out_complex && !out_soa ? 2 : 1) * p->esize;
+    const int in_parts = in_soa ? 2 : 1, out_parts = out_soa ? 2 : 1;
+    const size_t in_bytes = in_part * in_parts * batch, out_bytes = out_part * out_parts * batch;
+    std::lock_guard<std::mutex> lock(p->mu);
+    DeviceGuard g(p->device);
+    const bool pin_in = is_pinned(in0) && (!in_soa || is_pinned(in1));
+    const bool pin_out = is_pinned(out0) && (!out_soa || is_pinned(out1));
+    rc = ensure_staging(p, in_bytes, out_bytes);
+    if (rc) return rc;
+    // Device buffers: [part 0 of all transforms][part 1 of all transforms].
+    char* din = static_cast<char*>(p->d_in);
+    char* dout = static_cast<char*>(p->d_out);
+    const void* src[2] = {in0, in1};
+    void* dst[2] = {out0, out1};
+    if (!pin_in) {
+        for (int q = 0; q < in_parts; ++q)
+            memcpy(static_cast<char*>(p->h_in) + q * in_part * batch, src[q], in_part * batch);
+    }
+    // Chunking: about 16 MiB of input per chunk, at least one transform.
+    size_t chunk = (16u << 20) / (in_part * in_parts);
+    if (chunk == 0) chunk = 1;
+    if (chunk > batch) chunk = batch;
+    cudaStream_t ss[2] = {p->stream, p->stream2};
+    for (size_t b0 = 0, c = 0; b0 < batch; b0 += chunk, ++c) {
+        const size_t nb = (batch - b0 < chunk) ? batch - b0 : chunk;
+        cudaStream_t st = ss[c & 1];
+        for (int q = 0; q < in_parts; ++q) {
+            const char* h = pin_in ? static_cast<const char*>(src[q]) : static_cast<const char*>(p->h_in) + q * in_part * batch;
+            ZL_CUDA(cudaMemcpyAsync(din + q * in_part * batch + b0 * in_part, h + b0 * in_part, nb * in_part,
+                                    cudaMemcpyHostToDevice, st));
+        }
+        const void* i0 = din + b0 * in_part;
+        const void* i1 = in_soa ? din + in_part * batch + b0 * in_part : nullptr;
+        void* o0 = dout + b0 * out_part;
+        void* o1 = out_soa ? dout + out_part * batch + b0 * out_part : nullptr;
+        // dense strides: the device buffers hold whole transforms back to back
+        rc = exec_device_impl(p, op, in_layout, out_layout, i0, i1, o0, o1, nb, 0, 0, st);
+        if (rc) return rc;
+        for (int q = 0; q < out_parts; ++q) {
+            char* h = pin_out ? static_cast<char*>(dst[q]) : static_cast<char*>(p->h_out) + q * out_part * batch;
+            ZL_CUDA(cudaMemcpyAsync(h + b0 * out_part, dout + q * out_part * batch + b0 * out_part, nb * out_part,
+                                    cudaMemcpyDeviceToHost, st));
+        }
+    }
+    ZL_CUDA(cudaStreamSynchronize(ss[0]));
+    ZL_CUDA(cudaStreamSynchronize(ss[1]));
+    if (!pin_out) {
+        for (int q = 0; q < out_parts; ++q)
+            memcpy(dst[q], static_cast<char*>(p->h_out) + q * out_part * batch, out_part * batch);
+    }
+    return ZLFFT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, int mode, int device) {
+    if (!out) return fail(ZLFFT_ERR_INVALID_ARG, "plan pointer is null");
+    *out = nullptr;
+    if (kind != ZLFFT_C2C && kind != ZLFFT_R2C) return fail(ZLFFT_ERR_INVALID_ARG, "invalid kind %d", kind);
+    if (precision != ZLFFT_F32 && precision != ZLFFT_F64)
+        return fail(ZLFFT_ERR_INVALID_ARG, "invalid precision %d", precision);
+    if (order > 30) return fail(ZLFFT_ERR_INVALID_ARG, "order %zu out of range", order);
+    if (kind == ZLFFT_R2C && order < 1)
+        return fail(ZLFFT_ERR_INVALID_ARG, "RFFT order must be >= 1 (the reference underflows at 0)");
+    if (mode != ZLFFT_MODE_PLAIN) return fail(ZLFFT_ERR_UNSUPPORTED, "mode %d not available", mode);
+    const int cfft_order = kind == ZLFFT_C2C ? (int)order : (int)order - 1;
+    if (cfft_order > zlfft::kTileMaxP) return fail(ZLFFT_ERR_UNSUPPORTED, "order %zu not supported yet", order);
+
+    auto* p = new zlfft_plan_s();
+    p->kind = kind;
+    p->prec = precision;
+    p->order = (int)order;
+    p->cfft_order = cfft_order;
+    p->mode = mode;
+    p->esize = precision == ZLFFT_F32 ? 4 : 8;
+    if (device < 0) {
+        if (cudaGetDevice(&device) != cudaSuccess) {
+            delete p;
+            return fail(ZLFFT_ERR_CUDA, "no CUDA device");
+        }
+    }
+    p->device = device;
+    DeviceGuard g(device);
+    cudaError_t e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        release(p);
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    }
+    e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->stream2, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        release(p);
+        return cuda_fail(e, "cudaStreamCreate");
+    }
+    (void)tables();
+
+    const long long m = 1LL << cfft_order;
+    p->tw_count = (size_t)(3 * m / 4);
+    const size_t cx_bytes = 2 * p->esize;
+    e = cudaMalloc(&p->d_tw, (p->tw_count + 1) * cx_bytes);
+    if (e != cudaSuccess) {
+        release(p);
+        return fail(ZLFFT_ERR_ALLOC, "twiddle allocation failed");
+    }
+    if (p->tw_count > 0) {
+        const unsigned blocks = (unsigned)((p->tw_count + 255) / 256);
+        if (precision == ZLFFT_F32)
+            twiddle_kernel<float><<<blocks, 256, 0, p->stream>>>(static_cast<float2*>(p->d_tw), cfft_order,
+                                                                 (long long)p->tw_count);
+        else
+            twiddle_kernel<double><<<blocks, 256, 0, p->stream>>>(static_cast<double2*>(p->d_tw), cfft_order,
+                                                                  (long long)p->tw_count);
+    }
+    if (kind == ZLFFT_R2C) {
+        const long long cnt = m / 2 + 1;
+        if (cudaMalloc(&p->d_rwc, cnt * p->esize) != cudaSuccess || cudaMalloc(&p->d_rws, cnt * p->esize) != cudaSuccess) {
+            release(p);
+            return fail(ZLFFT_ERR_ALLOC, "RFFT twiddle allocation failed");
+        }
+        const unsigned blocks = (unsigned)((cnt + 255) / 256);
+        if (precision == ZLFFT_F32)
+            rfft_twiddle_kernel<float><<<blocks, 256, 0, p->stream>>>(static_cast<float*>(p->d_rwc),
+                                                                      static_cast<float*>(p->d_rws), (int)order, cnt);
+        else
+            rfft_twiddle_kernel<double><<<blocks, 256, 0, p->stream>>>(static_cast<double*>(p->d_rwc),
+                                                                       static_cast<double*>(p->d_rws), (int)order, cnt);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+    if (e != cudaSuccess) {
+        release(p);
+        return cuda_fail(e, "twiddle generation");
+    }
+    *out = p;
+    return ZLFFT_OK;
+}
+
+int zlfft_plan_destroy(zlfft_plan plan) {
+    release(plan);
+    return ZLFFT_OK;
+}
+
+int zlfft_plan_get_size(zlfft_plan plan, size_t* size) {
+    if (!plan || !size) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    *size = size_t{1} << plan->order;
+    return ZLFFT_OK;
+}
+
+int zlfft_plan_get_order(zlfft_plan plan, size_t* order) {
+    if (!plan || !order) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    *order = (size_t)plan->order;
+    return ZLFFT_OK;
+}
+
+int zlfft_exec_host(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0, const void* in1,
+                    void* out0, void* out1) {
+    if (!plan) return fail(ZLFFT_ERR_INVALID_ARG, "null plan");
+    return exec_host_impl(plan, op, in_layout, out_layout, in0, in1, out0, out1, 1);
+}
+
+int zlfft_exec_host_batched(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0,
+                            const void* in1, void* out0, void* out1, size_t batch) {
+    if (!plan) return fail(ZLFFT_ERR_INVALID_ARG, "null plan");
+    return exec_host_impl(plan, op, in_layout, out_layout, in0, in1, out0, out1, batch);
+}
+
+int zlfft_exec_device(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0, const void* in1,
+                      void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, void* stream) {
+    if (!plan) return fail(ZLFFT_ERR_INVALID_ARG, "null plan");
+    return exec_device_impl(plan, op, in_layout, out_layout, in0, in1, out0, out1, batch, in_stride, out_stride,
+                            static_cast<cudaStream_t>(stream));
+}
+
+int zlfft_plan_take_launch_count(zlfft_plan plan, size_t* launches) {
+    if (!plan || !launches) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    *launches = plan->launches;
+    plan->launches = 0;
+    return ZLFFT_OK;
+}
+
+int zlfft_plan_copy_twiddles(zlfft_plan plan, void* host_out, size_t capacity_elems, size_t* count) {
+    if (!plan || !count) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    *count = plan->tw_count;
+    if (!host_out) return ZLFFT_OK;
+    if (capacity_elems < plan->tw_count) return fail(ZLFFT_ERR_INVALID_ARG, "capacity too small");
+    DeviceGuard g(plan->device);
+    ZL_CUDA(cudaMemcpy(host_out, plan->d_tw, plan->tw_count * 2 * plan->esize, cudaMemcpyDeviceToHost));
+    return ZLFFT_OK;
+}
+
+const char* zlfft_last_error(void) { return g_last_error.c_str(); }
+
+const char* zlfft_version(void) { return "zlfft-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

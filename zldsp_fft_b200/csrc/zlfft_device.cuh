@@ -1,0 +1,150 @@
+// Device building blocks shared by every FFT kernel of libzlfft_cuda.
+//
+// Arithmetic follows the reference's rounding exactly: each MulAdd/NegMulAdd
+// of the reference is one fma here, every other multiply is an explicitly
+// rounded multiply (__fmul_rn/__dmul_rn), which the compiler never contracts
+// into a neighbouring add. With the same twiddle bits, a plain-form kernel
+// therefore reproduces the reference's micro-only Stockham output bit for bit.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace zlfft {
+
+template <typename F>
+struct CxT;
+template <>
+struct CxT<float> {
+    using type = float2;
+};
+template <>
+struct CxT<double> {
+    using type = double2;
+};
+template <typename F>
+using Cx = typename CxT<F>::type;
+
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+template <typename C>
+__device__ __forceinline__ C cx(decltype(C::x) r, decltype(C::x) i) {
+    C c;
+    c.x = r;
+    c.y = i;
+    return c;
+}
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) {
+    return cx<C>(a.x + b.x, a.y + b.y);
+}
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) {
+    return cx<C>(a.x - b.x, a.y - b.y);
+}
+// a - i*b
+template <typename C>
+__device__ __forceinline__ C csub_i(C a, C b) {
+    return cx<C>(a.x + b.y, a.y - b.x);
+}
+// a + i*b
+template <typename C>
+__device__ __forceinline__ C cadd_i(C a, C b) {
+    return cx<C>(a.x - b.y, a.y + b.x);
+}
+// x * w: re = fma(-xi, wi, xr*wr), im = fma(xi, wr, xr*wi)
+// (src/common/zldsp_fft_common_radix.hpp:114-115 of the reference).
+template <typename C>
+__device__ __forceinline__ C cmul_tw(C x, C w) {
+    return cx<C>(fma_rn(-x.y, w.y, mul_rn(x.x, w.x)), fma_rn(x.y, w.x, mul_rn(x.x, w.y)));
+}
+// Swap re/im: the reference's backward transform is swap(DFT(swap(x)))
+// (src/common/zldsp_fft_common_structure.hpp:47-95).
+template <typename C>
+__device__ __forceinline__ C cswap(C a) {
+    return cx<C>(a.y, a.x);
+}
+
+// Radix-4 butterfly of the first Stockham pass (no twiddles), in place:
+// a_q = x[j + q*N/4] in, a_m = DFT4 output m out
+// (src/common/zldsp_fft_common_radix.hpp:192-238).
+template <typename C>
+__device__ __forceinline__ void bfly4_first(C& a0, C& a1, C& a2, C& a3) {
+    const C t0 = cadd(a0, a2), t1 = csub(a0, a2);
+    const C t2 = cadd(a1, a3), t3 = csub(a1, a3);
+    a0 = cadd(t0, t2);
+    a1 = csub_i(t1, t3);
+    a2 = csub(t0, t2);
+    a3 = cadd_i(t1, t3);
+}
+
+// Twiddled radix-4 DIT butterfly, in place (src/common/zldsp_fft_common_radix.hpp:103-156).
+template <typename C>
+__device__ __forceinline__ void bfly4_tw(C& a0, C& a1, C& a2, C& a3, C w1, C w2, C w3) {
+    const C t1 = cmul_tw(a1, w1);
+    const C t3 = cmul_tw(a3, w3);
+    const C s2 = cadd(t1, t3), s3 = csub(t1, t3);
+    const C t2 = cmul_tw(a2, w2);
+    const C s0 = cadd(a0, t2), s1 = csub(a0, t2);
+    a0 = cadd(s0, s2);
+    a1 = csub_i(s1, s3);
+    a2 = csub(s0, s2);
+    a3 = cadd_i(s1, s3);
+}
+
+// Radix-8 butterfly of the first Stockham pass, in place: a_q = x[j + q*N/8]
+// in, a_p = DFT8 output p out. The W8 factors use 1/sqrt(2) formed as the
+// double quotient rounded to F (src/common/zldsp_fft_common_radix.hpp:495-568).
+template <typename C>
+__device__ __forceinline__ void bfly8_first(C* a) {
+    using F = decltype(C::x);
+    const F c = (F)(1.0 / 1.4142135623730951);
+    const C t0 = cadd(a[0], a[4]), t1 = csub(a[0], a[4]);
+    const C t2 = cadd(a[2], a[6]), t3 = csub(a[2], a[6]);
+    const C y00 = cadd(t0, t2), y02 = csub(t0, t2);
+    const C y01 = csub_i(t1, t3), y03 = cadd_i(t1, t3);
+    const C u0 = cadd(a[1], a[5]), u1 = csub(a[1], a[5]);
+    const C u2 = cadd(a[3], a[7]), u3 = csub(a[3], a[7]);
+    const C y10 = cadd(u0, u2), y12 = csub(u0, u2);
+    const C y11 = csub_i(u1, u3), y13 = cadd_i(u1, u3);
+    const C v1 = cx<C>(mul_rn(y11.x + y11.y, c), mul_rn(y11.y - y11.x, c));
+    const C v2 = cx<C>(y12.y, -y12.x);
+    const C v3 = cx<C>(mul_rn(y13.y - y13.x, c), mul_rn(-(y13.x + y13.y), c));
+    a[0] = cadd(y00, y10);
+    a[1] = cadd(y01, v1);
+    a[2] = cadd(y02, v2);
+    a[3] = cadd(y03, v3);
+    a[4] = csub(y00, y10);
+    a[5] = csub(y01, v1);
+    a[6] = csub(y02, v2);
+    a[7] = csub(y03, v3);
+}
+
+template <typename C>
+__device__ __forceinline__ void bfly2(C& a0, C& a1) {
+    const C t = a0;
+    a0 = cadd(t, a1);
+    a1 = csub(t, a1);
+}
+
+// Twiddle W_N^t from the unified table T[t] = exp(-2*pi*i*t/N), t < 3N/4
+// (a plain cached load: the table is shared by every CTA and stays in L1/L2;
+// unlike the non-coherent path it is not hoisted across barriers).
+template <typename C>
+__device__ __forceinline__ C tw_load(const C* tw, uint32_t t) {
+    return tw[t];
+}
+
+// Shared-memory padding: one spare slot per 128 bytes, so that the strided
+// writes of a Stockham exchange fall in distinct banks.
+template <typename C>
+struct SmemPad {
+    static constexpr int kShift = sizeof(C) == 8 ? 4 : 3;  // 16 float2 or 8 double2 per 128 B
+    __device__ __host__ static constexpr uint32_t idx(uint32_t p) { return p + (p >> kShift); }
+    __device__ __host__ static constexpr uint32_t size(uint32_t n) { return n + (n >> kShift) + 1; }
+};
+
+}  // namespace zlfft

@@ -1,0 +1,93 @@
+// Launch tables: every (precision, order, operation, layout) kernel variant is
+// instantiated once at build time and reached through a table of launch
+// functions, so the C ABI dispatches with one indexed load.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "zlfft_tile.cuh"
+
+namespace zlfft {
+
+constexpr int kTileMaxP_f32 = 13;  // tile kernel: whole transform in one CTA
+constexpr int kTileMaxP_f64 = 13;
+constexpr int kTileMaxP = 13;
+
+struct LaunchCtx {
+    int num_sms;
+    size_t* launches;  // incremented per kernel launch
+};
+
+using TileLaunchFn = cudaError_t (*)(const TileArgs&, cudaStream_t, const LaunchCtx&);
+
+struct TileTable {
+    // [order][op][in_layout][out_layout]
+    TileLaunchFn fn[kTileMaxP + 1][5][2][2];
+};
+
+template <typename F, int P, int OP, int IL, int OL>
+cudaError_t launch_tile(const TileArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
+    using Cfg = TileCfg<F, P>;
+    auto kern = tile_kernel<F, P, OP, IL, OL>;
+    static const int blocks_per_sm = [kern]() {
+        if (Cfg::SMEM > 48 * 1024) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+        }
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, Cfg::THREADS, Cfg::SMEM) != cudaSuccess || b < 1) {
+            b = 1;
+        }
+        return b;
+    }();
+    if (a.batch <= 0) return cudaSuccess;
+    const long long tiles = (a.batch + Cfg::TPC - 1) / Cfg::TPC;
+    const long long cap = (long long)ctx.num_sms * blocks_per_sm;
+    const unsigned grid = (unsigned)(tiles < cap ? tiles : cap);
+    kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(a);
+    if (ctx.launches) ++*ctx.launches;
+    return cudaGetLastError();
+}
+
+// Each translation unit fills its part of a precision's table.
+void fill_tile_c2c_f32(TileTable& t);
+void fill_tile_r2c_f32(TileTable& t);
+void fill_tile_c2c_f64(TileTable& t);
+void fill_tile_r2c_f64(TileTable& t);
+
+template <typename F, int P>
+void fill_tile_c2c_order(TileTable& t) {
+    t.fn[P][kC2CFwd][kAoS][kAoS] = launch_tile<F, P, kC2CFwd, kAoS, kAoS>;
+    t.fn[P][kC2CFwd][kAoS][kSoA] = launch_tile<F, P, kC2CFwd, kAoS, kSoA>;
+    t.fn[P][kC2CFwd][kSoA][kAoS] = launch_tile<F, P, kC2CFwd, kSoA, kAoS>;
+    t.fn[P][kC2CFwd][kSoA][kSoA] = launch_tile<F, P, kC2CFwd, kSoA, kSoA>;
+    t.fn[P][kC2CBwd][kAoS][kAoS] = launch_tile<F, P, kC2CBwd, kAoS, kAoS>;
+    t.fn[P][kC2CBwd][kAoS][kSoA] = launch_tile<F, P, kC2CBwd, kAoS, kSoA>;
+    t.fn[P][kC2CBwd][kSoA][kAoS] = launch_tile<F, P, kC2CBwd, kSoA, kAoS>;
+    t.fn[P][kC2CBwd][kSoA][kSoA] = launch_tile<F, P, kC2CBwd, kSoA, kSoA>;
+}
+
+// R2C/C2R: P is the inner CFFT order (real length 2^(P+1)). The real side has
+// no layout; both layout slots of that side point at the same kernel.
+template <typename F, int P>
+void fill_tile_r2c_order(TileTable& t) {
+    for (int il = 0; il < 2; ++il) {
+        t.fn[P][kR2CFwd][il][kAoS] = launch_tile<F, P, kR2CFwd, kAoS, kAoS>;
+        t.fn[P][kR2CFwd][il][kSoA] = launch_tile<F, P, kR2CFwd, kAoS, kSoA>;
+        for (int ol = 0; ol < 2; ++ol) t.fn[P][kR2CSqrMag][il][ol] = launch_tile<F, P, kR2CSqrMag, kAoS, kAoS>;
+    }
+    for (int ol = 0; ol < 2; ++ol) {
+        t.fn[P][kC2RBwd][kAoS][ol] = launch_tile<F, P, kC2RBwd, kAoS, kAoS>;
+        t.fn[P][kC2RBwd][kSoA][ol] = launch_tile<F, P, kC2RBwd, kSoA, kAoS>;
+    }
+}
+
+template <typename F, int... Ps>
+void fill_c2c_orders(TileTable& t, std::integer_sequence<int, Ps...>) {
+    (fill_tile_c2c_order<F, Ps>(t), ...);
+}
+template <typename F, int... Ps>
+void fill_r2c_orders(TileTable& t, std::integer_sequence<int, Ps...>) {
+    (fill_tile_r2c_order<F, Ps>(t), ...);
+}
+
+}  // namespace zlfft

@@ -1,0 +1,199 @@
+"""Host-side mirror of the reference's operator interface.
+
+``CFFT`` and ``RFFT`` have the constructors, getters and forward/backward
+member functions of zldsp::fft::CFFT<F> (src/zldsp_fft_cfft.hpp:11-118) and
+zldsp::fft::RFFT<F> (src/zldsp_fft_rfft.hpp:11-139), taking numpy host
+buffers: an AoS complex buffer is a complex ndarray, a split-SoA buffer is a
+pair ``(re, im)`` of real ndarrays, exactly the reference's
+``std::complex<F>*`` / ``std::array<F*, 2>`` overloads. Calls are synchronous
+and write into the caller's output buffers, like the reference.
+
+``Plan`` is the batched device-pointer entry point (zlfft_exec_device) for
+callers that keep data in GPU memory (raw pointers or torch CUDA tensors).
+
+Everything runs on the GPU through libzlfft_cuda.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+
+
+def _prec(dtype) -> int:
+    dt = np.dtype(dtype)
+    if dt in (np.float32, np.complex64):
+        return C.F32
+    if dt in (np.float64, np.complex128):
+        return C.F64
+    raise TypeError(f"unsupported dtype {dt}; the reference is instantiated for float and double")
+
+
+class Plan:
+    """A zlfft plan (one transform size, kind, precision and form)."""
+
+    def __init__(self, kind: int, order: int, dtype=np.float32, mode: int = C.MODE_PLAIN, device: int = -1):
+        self._lib = C.lib()
+        self.kind = kind
+        self.order = int(order)
+        self.prec = _prec(dtype)
+        self.mode = mode
+        h = ctypes.c_void_p()
+        C.check(self._lib.zlfft_plan_create(ctypes.byref(h), kind, self.prec, self.order, mode, device))
+        self.handle = h
+
+    @property
+    def real_dtype(self):
+        return np.float32 if self.prec == C.F32 else np.float64
+
+    @property
+    def complex_dtype(self):
+        return np.complex64 if self.prec == C.F32 else np.complex128
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            self._lib.zlfft_plan_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_size(self) -> int:
+        v = ctypes.c_size_t()
+        C.check(self._lib.zlfft_plan_get_size(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def get_order(self) -> int:
+        v = ctypes.c_size_t()
+        C.check(self._lib.zlfft_plan_get_order(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def exec_device(self, op, in_layout, out_layout, in0, in1, out0, out1, batch, in_stride=0, out_stride=0,
+                    stream=0):
+        """Batched transform on device pointers (ints), async on `stream` (cudaStream_t as int)."""
+        C.check(self._lib.zlfft_exec_device(self.handle, op, in_layout, out_layout, in0, in1, out0, out1,
+                                            int(batch), int(in_stride), int(out_stride), stream))
+
+    def exec_host(self, op, in_layout, out_layout, in0, in1, out0, out1, batch=1):
+        C.check(self._lib.zlfft_exec_host_batched(self.handle, op, in_layout, out_layout, in0, in1, out0, out1,
+                                                  int(batch)))
+
+    def take_launch_count(self) -> int:
+        v = ctypes.c_size_t()
+        C.check(self._lib.zlfft_plan_take_launch_count(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def twiddles(self) -> np.ndarray:
+        """The device-generated unified twiddle table, copied to the host."""
+        n = ctypes.c_size_t()
+        C.check(self._lib.zlfft_plan_copy_twiddles(self.handle, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), self.complex_dtype)
+        C.check(self._lib.zlfft_plan_copy_twiddles(self.handle, out.ctypes.data, out.size, ctypes.byref(n)))
+        return out[: n.value]
+
+
+def _complex_arg(buf, n, cdt, rdt, name, writable):
+    """(layout, ptr0, ptr1) for an AoS ndarray or an SoA (re, im) pair."""
+    if isinstance(buf, (tuple, list)):
+        if len(buf) != 2:
+            raise ValueError(f"{name}: SoA buffer must be a (re, im) pair")
+        re, im = buf
+        for a in (re, im):
+            if not isinstance(a, np.ndarray) or a.dtype != rdt or not a.flags.c_contiguous or a.size < n:
+                raise ValueError(f"{name}: SoA parts must be contiguous {np.dtype(rdt)} arrays of >= {n} elements")
+            if writable and not a.flags.writeable:
+                raise ValueError(f"{name}: output is read-only")
+        return C.SOA, re.ctypes.data, im.ctypes.data
+    if not isinstance(buf, np.ndarray) or buf.dtype != cdt or not buf.flags.c_contiguous or buf.size < n:
+        raise ValueError(f"{name}: AoS buffer must be a contiguous {np.dtype(cdt)} array of >= {n} elements")
+    if writable and not buf.flags.writeable:
+        raise ValueError(f"{name}: output is read-only")
+    return C.AOS, buf.ctypes.data, None
+
+
+def _real_arg(buf, n, rdt, name, writable):
+    if not isinstance(buf, np.ndarray) or buf.dtype != rdt or not buf.flags.c_contiguous or buf.size < n:
+        raise ValueError(f"{name}: must be a contiguous {np.dtype(rdt)} array of >= {n} elements")
+    if writable and not buf.flags.writeable:
+        raise ValueError(f"{name}: output is read-only")
+    return buf.ctypes.data
+
+
+class CFFT:
+    """zldsp::fft::CFFT<F> on the GPU (src/zldsp_fft_cfft.hpp:11-118).
+
+    forward/backward(in, out) accept the reference's four layout pairings:
+    AoS->AoS, AoS->SoA, SoA->AoS, SoA->SoA. backward is the unnormalised
+    inverse (backward(forward(x)) == N * x)."""
+
+    def __init__(self, order: int, dtype=np.float32, mode: int = C.MODE_PLAIN):
+        self._plan = Plan(C.C2C, order, dtype, mode)
+        self._n = 1 << int(order)
+
+    def get_size(self) -> int:
+        return self._plan.get_size()
+
+    def get_order(self) -> int:
+        return self._plan.get_order()
+
+    def _exec(self, op, in_buffer, out_buffer):
+        p = self._plan
+        il, i0, i1 = _complex_arg(in_buffer, self._n, p.complex_dtype, p.real_dtype, "in_buffer", False)
+        ol, o0, o1 = _complex_arg(out_buffer, self._n, p.complex_dtype, p.real_dtype, "out_buffer", True)
+        p.exec_host(op, il, ol, i0, i1, o0, o1)
+
+    def forward(self, in_buffer, out_buffer) -> None:
+        self._exec(C.FORWARD, in_buffer, out_buffer)
+
+    def backward(self, in_buffer, out_buffer) -> None:
+        self._exec(C.BACKWARD, in_buffer, out_buffer)
+
+    @property
+    def plan(self) -> Plan:
+        return self._plan
+
+
+class RFFT:
+    """zldsp::fft::RFFT<F> on the GPU (src/zldsp_fft_rfft.hpp:11-139).
+
+    forward(real_in, out) writes N/2+1 bins (AoS ndarray or SoA pair);
+    backward(in, real_out) is unnormalised (backward(forward(x)) == N/2 * x);
+    forward_sqr_mag(real_in, out) writes N/2+1 squared magnitudes."""
+
+    def __init__(self, order: int, dtype=np.float32, mode: int = C.MODE_PLAIN):
+        self._plan = Plan(C.R2C, order, dtype, mode)
+        self._n = 1 << int(order)
+        self._nb = self._n // 2 + 1
+
+    def get_size(self) -> int:
+        return self._plan.get_size()
+
+    def get_order(self) -> int:
+        return self._plan.get_order()
+
+    def forward(self, in_buffer, out_buffer) -> None:
+        p = self._plan
+        i0 = _real_arg(in_buffer, self._n, p.real_dtype, "in_buffer", False)
+        ol, o0, o1 = _complex_arg(out_buffer, self._nb, p.complex_dtype, p.real_dtype, "out_buffer", True)
+        p.exec_host(C.FORWARD, C.AOS, ol, i0, None, o0, o1)
+
+    def backward(self, in_buffer, out_buffer) -> None:
+        p = self._plan
+        il, i0, i1 = _complex_arg(in_buffer, self._nb, p.complex_dtype, p.real_dtype, "in_buffer", False)
+        o0 = _real_arg(out_buffer, self._n, p.real_dtype, "out_buffer", True)
+        p.exec_host(C.BACKWARD, il, C.AOS, i0, i1, o0, None)
+
+    def forward_sqr_mag(self, in_buffer, out_buffer) -> None:
+        p = self._plan
+        i0 = _real_arg(in_buffer, self._n, p.real_dtype, "in_buffer", False)
+        o0 = _real_arg(out_buffer, self._nb, p.real_dtype, "out_buffer", True)
+        p.exec_host(C.FORWARD_SQR_MAG, C.AOS, C.AOS, i0, None, o0, None)
+
+    @property
+    def plan(self) -> Plan:
+        return self._plan
