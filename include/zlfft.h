@@ -118,8 +118,8 @@ ZLFFT_API int zlfft_exec_host_batched(zlfft_plan plan, int op, int in_layout, in
 ZLFFT_API int zlfft_exec_device(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0, const void* in1,
                       void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, void* stream);
 
-/* Number of CUDA kernels launched by this plan on the calling thread since
- * the last call (diagnostics for benchmarks). */
+/* Number of CUDA kernels this plan has launched since the previous call
+ * (diagnostics for benchmarks). */
 ZLFFT_API int zlfft_plan_take_launch_count(zlfft_plan plan, size_t* launches);
 
 /* Copy the plan's unified twiddle table T[t] = exp(-2 pi i t / M), t < 3M/4,
@@ -127,6 +127,20 @@ ZLFFT_API int zlfft_plan_take_launch_count(zlfft_plan plan, size_t* launches);
  * re/im pairs of the plan precision. `count` receives 3M/4. Diagnostics: lets
  * a caller compare the device-generated table with the reference's. */
 ZLFFT_API int zlfft_plan_copy_twiddles(zlfft_plan plan, void* host_out, size_t capacity_elems, size_t* count);
+
+/* Synchronise the plan's device, then read and clear the plan's device error
+ * word. Kernels bound every wait they perform (on a TMA completion barrier or
+ * on another CTA's progress); a wait that runs out of its iteration limit
+ * sets a bit here and the kernel returns early instead of hanging the GPU.
+ * Returns ZLFFT_ERR_DEVICE_TIMEOUT if *status != 0. No reference counterpart
+ * (the reference runs on one CPU thread and never waits). */
+ZLFFT_API int zlfft_plan_device_status(zlfft_plan plan, int* status);
+
+/* Failure-detection self-test: runs one kernel that waits on a barrier that
+ * never completes, with a short poll limit, and returns in *status the error
+ * word the kernel left (kDevErrWaitTimeout = 1 when the bounded wait gave up
+ * as designed). The GPU context stays usable. No reference counterpart. */
+ZLFFT_API int zlfft_selftest_bounded_wait(int device, int* status);
 
 /* Message of the calling thread's last failure ("" if none). */
 ZLFFT_API const char* zlfft_last_error(void);

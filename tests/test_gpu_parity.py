@@ -234,3 +234,18 @@ def test_launch_counter():
         plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, x.data_ptr(), None, x.data_ptr(), None, 8)
     torch.cuda.synchronize()
     assert plan.take_launch_count() == 3
+
+
+def test_bounded_wait_reports_instead_of_hanging():
+    """A device wait that can never complete gives up after its poll limit,
+    sets the error word and returns; the context stays usable afterwards."""
+    import ctypes
+    lib = Z._capi.lib()
+    st = ctypes.c_int(-1)
+    Z._capi.check(lib.zlfft_selftest_bounded_wait(0, ctypes.byref(st)))
+    assert st.value == 1
+    plan = Z.Plan(Z.C2C, 8, np.float32)
+    assert plan.device_status() == 0
+    x = np.ones((2, 256), np.complex64)
+    y = G.run_c2c(plan, x, True)
+    assert y[0, 0] == 256

@@ -39,6 +39,8 @@ EXPORTS = (
     "zlfft_exec_device",
     "zlfft_plan_take_launch_count",
     "zlfft_plan_copy_twiddles",
+    "zlfft_plan_device_status",
+    "zlfft_selftest_bounded_wait",
     "zlfft_last_error",
     "zlfft_version",
 )
@@ -76,6 +78,8 @@ def lib() -> ctypes.CDLL:
         L.zlfft_exec_device.argtypes = [vp, i, i, i, vp, vp, vp, vp, sz, sz, sz, vp]
         L.zlfft_plan_take_launch_count.argtypes = [vp, ctypes.POINTER(sz)]
         L.zlfft_plan_copy_twiddles.argtypes = [vp, vp, sz, ctypes.POINTER(sz)]
+        L.zlfft_plan_device_status.argtypes = [vp, ctypes.POINTER(i)]
+        L.zlfft_selftest_bounded_wait.argtypes = [i, ctypes.POINTER(i)]
         L.zlfft_last_error.restype = ctypes.c_char_p
         L.zlfft_last_error.argtypes = []
         L.zlfft_version.restype = ctypes.c_char_p

@@ -64,16 +64,48 @@ __global__ void twiddle_kernel(zlfft::Cx<F>* tw, int order, long long count) {
     tw[t] = w;
 }
 
-// RFFT split twiddles k = 0..M/2 for real length Nr = 2M:
-// wc = 0.5*cos(2 pi k / Nr), ws = 0.5*sin(2 pi k / Nr) + 0.5, FP64 then rounded
-// (src/common/zldsp_fft_common_init.hpp:374-381). Index 0 is unused.
+// RFFT split twiddles k = 0..M/2 for real length Nr = 2M, stored as pairs
+// (wc, ws): wc = 0.5*cos(2 pi k / Nr), ws = 0.5*sin(2 pi k / Nr) + 0.5, FP64
+// then rounded (src/common/zldsp_fft_common_init.hpp:374-381). Index 0 unused.
 template <typename F>
-__global__ void rfft_twiddle_kernel(F* wc, F* ws, int rfft_order, long long count) {
+__global__ void rfft_twiddle_kernel(zlfft::Cx<F>* rw, int rfft_order, long long count) {
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const double a = (double)k * (2.0 / (double)(1LL << rfft_order));
-    wc[k] = (F)__dmul_rn(0.5, ref_cospi(a));
-    ws[k] = (F)__dadd_rn(__dmul_rn(0.5, ref_sinpi(a)), 0.5);
+    zlfft::Cx<F> w;
+    w.x = (F)__dmul_rn(0.5, ref_cospi(a));
+    w.y = (F)__dadd_rn(__dmul_rn(0.5, ref_sinpi(a)), 0.5);
+    rw[k] = w;
+}
+
+// Per-stage tables (layout in zlfft_tile.cuh, stage_l0): entry r of the stage
+// with sub-length L is W_{4L}^{q k} = T[q*k*M/(4L)] with q = r/L + 1, k = r%L,
+// copied from the unified table T so the bits are identical.
+template <typename F>
+__global__ void stage_table_kernel(zlfft::Cx<F>* tws, const zlfft::Cx<F>* tw, int order, long long count) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= count) return;
+    const long long l0 = zlfft::stage_l0(order);
+    long long L = l0;
+    while (4 * L - l0 <= idx) L *= 4;  // stage containing idx: offset L - l0, size 3L
+    const long long r = idx - (L - l0);
+    const long long q = r / L + 1, k = r % L;
+    const long long m = 1LL << order;
+    tws[idx] = tw[q * k * (m / (4 * L))];
+}
+
+// Self-test of the bounded-wait path: one CTA waits on an mbarrier that no
+// one ever arrives at, with a short poll limit; the wait gives up, the kernel
+// records kDevErrWaitTimeout in the error word and returns normally.
+__global__ void selftest_wait_kernel(int* err, uint32_t limit) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        zlfft::mbar_init(&bar, 1);
+        zlfft::fence_mbar_init();
+    }
+    __syncthreads();
+    const bool ok = zlfft::mbar_wait(&bar, 0, limit);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(err, zlfft::kDevErrWaitTimeout);
 }
 
 struct TablesHolder {
@@ -105,8 +137,8 @@ struct zlfft_plan_s {
     size_t esize = 0;  // bytes of one real
     void* d_tw = nullptr;
     size_t tw_count = 0;
-    void* d_rwc = nullptr;
-    void* d_rws = nullptr;
+    void* d_tws = nullptr;  // per-stage twiddle tables
+    void* d_rw = nullptr;   // RFFT split twiddle pairs
     // host staging
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;
@@ -116,6 +148,7 @@ struct zlfft_plan_s {
     void* d_out = nullptr;
     size_t stage_in_bytes = 0, stage_out_bytes = 0;
     size_t launches = 0;
+    int* d_err = nullptr;  // device error word written by kernels (bounded waits that ran out)
     std::mutex mu;
 };
 
@@ -136,8 +169,9 @@ void release(zlfft_plan p) {
     if (!p) return;
     DeviceGuard g(p->device);
     if (p->d_tw) cudaFree(p->d_tw);
-    if (p->d_rwc) cudaFree(p->d_rwc);
-    if (p->d_rws) cudaFree(p->d_rws);
+    if (p->d_tws) cudaFree(p->d_tws);
+    if (p->d_rw) cudaFree(p->d_rw);
+    if (p->d_err) cudaFree(p->d_err);
     if (p->d_in) cudaFree(p->d_in);
     if (p->d_out) cudaFree(p->d_out);
     if (p->h_in) cudaFreeHost(p->h_in);
@@ -222,8 +256,17 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     a.in_stride = (long long)(ex.in_complex ? in_stride : in_stride / 2);
     a.out_stride = (long long)((ex.out_complex || op == ZLFFT_FORWARD_SQR_MAG) ? out_stride : out_stride / 2);
     a.tw = p->d_tw;
-    a.rwc = p->d_rwc;
-    a.rws = p->d_rws;
+    a.tws = p->d_tws;
+    a.rw = p->d_rw;
+    a.err = p->d_err;
+    // Bulk (TMA) copies need 16-byte aligned sources: the bases and the
+    // per-transform stride in bytes. The kernel reads directly otherwise.
+    {
+        const size_t in_elem_bytes = in_soa ? p->esize : 2 * p->esize;  // complex or pairs of reals
+        const bool al = aligned(in0, 16) && (!in_soa || aligned(in1, 16)) &&
+                        (batch == 1 || ((size_t)a.in_stride * in_elem_bytes) % 16 == 0);
+        a.tma = al ? 1 : 0;
+    }
 
     const int dop = device_op_code(p, op);
     const int P = p->cfft_order;
@@ -332,6 +375,14 @@ int exec_host_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const
     }
     ZL_CUDA(cudaStreamSynchronize(ss[0]));
     ZL_CUDA(cudaStreamSynchronize(ss[1]));
+    {
+        int derr = 0;
+        ZL_CUDA(cudaMemcpy(&derr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (derr) {
+            cudaMemset(p->d_err, 0, sizeof(int));
+            return fail(ZLFFT_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration limit (code %d)", derr);
+        }
+    }
     if (!pin_out) {
         for (int q = 0; q < out_parts; ++q)
             memcpy(dst[q], static_cast<char*>(p->h_out) + q * out_part * batch, out_part * batch);
@@ -383,6 +434,10 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
         return cuda_fail(e, "cudaStreamCreate");
     }
     (void)tables();
+    if (cudaMalloc(&p->d_err, sizeof(int)) != cudaSuccess || cudaMemset(p->d_err, 0, sizeof(int)) != cudaSuccess) {
+        release(p);
+        return fail(ZLFFT_ERR_ALLOC, "error-word allocation failed");
+    }
 
     const long long m = 1LL << cfft_order;
     p->tw_count = (size_t)(3 * m / 4);
@@ -401,19 +456,36 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
             twiddle_kernel<double><<<blocks, 256, 0, p->stream>>>(static_cast<double2*>(p->d_tw), cfft_order,
                                                                   (long long)p->tw_count);
     }
+    // per-stage tables: N - L0 entries (the stages with sub-length L0 .. N/4)
+    {
+        const long long l0 = zlfft::stage_l0(cfft_order);
+        const long long cnt = m >= 4 * l0 ? m - l0 : 0;
+        if (cudaMalloc(&p->d_tws, (size_t)(cnt + 1) * cx_bytes) != cudaSuccess) {
+            release(p);
+            return fail(ZLFFT_ERR_ALLOC, "twiddle allocation failed");
+        }
+        if (cnt > 0) {
+            const unsigned blocks = (unsigned)((cnt + 255) / 256);
+            if (precision == ZLFFT_F32)
+                stage_table_kernel<float><<<blocks, 256, 0, p->stream>>>(
+                    static_cast<float2*>(p->d_tws), static_cast<const float2*>(p->d_tw), cfft_order, cnt);
+            else
+                stage_table_kernel<double><<<blocks, 256, 0, p->stream>>>(
+                    static_cast<double2*>(p->d_tws), static_cast<const double2*>(p->d_tw), cfft_order, cnt);
+        }
+    }
     if (kind == ZLFFT_R2C) {
         const long long cnt = m / 2 + 1;
-        if (cudaMalloc(&p->d_rwc, cnt * p->esize) != cudaSuccess || cudaMalloc(&p->d_rws, cnt * p->esize) != cudaSuccess) {
+        if (cudaMalloc(&p->d_rw, cnt * cx_bytes) != cudaSuccess) {
             release(p);
             return fail(ZLFFT_ERR_ALLOC, "RFFT twiddle allocation failed");
         }
         const unsigned blocks = (unsigned)((cnt + 255) / 256);
         if (precision == ZLFFT_F32)
-            rfft_twiddle_kernel<float><<<blocks, 256, 0, p->stream>>>(static_cast<float*>(p->d_rwc),
-                                                                      static_cast<float*>(p->d_rws), (int)order, cnt);
+            rfft_twiddle_kernel<float><<<blocks, 256, 0, p->stream>>>(static_cast<float2*>(p->d_rw), (int)order, cnt);
         else
-            rfft_twiddle_kernel<double><<<blocks, 256, 0, p->stream>>>(static_cast<double*>(p->d_rwc),
-                                                                       static_cast<double*>(p->d_rws), (int)order, cnt);
+            rfft_twiddle_kernel<double><<<blocks, 256, 0, p->stream>>>(static_cast<double2*>(p->d_rw), (int)order,
+                                                                       cnt);
     }
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
@@ -475,6 +547,29 @@ int zlfft_plan_copy_twiddles(zlfft_plan plan, void* host_out, size_t capacity_el
     if (capacity_elems < plan->tw_count) return fail(ZLFFT_ERR_INVALID_ARG, "capacity too small");
     DeviceGuard g(plan->device);
     ZL_CUDA(cudaMemcpy(host_out, plan->d_tw, plan->tw_count * 2 * plan->esize, cudaMemcpyDeviceToHost));
+    return ZLFFT_OK;
+}
+
+int zlfft_plan_device_status(zlfft_plan plan, int* status) {
+    if (!plan || !status) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard g(plan->device);
+    ZL_CUDA(cudaDeviceSynchronize());
+    ZL_CUDA(cudaMemcpy(status, plan->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    ZL_CUDA(cudaMemset(plan->d_err, 0, sizeof(int)));
+    return *status ? ZLFFT_ERR_DEVICE_TIMEOUT : ZLFFT_OK;
+}
+
+int zlfft_selftest_bounded_wait(int device, int* status) {
+    if (!status) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard g(device);
+    int* d = nullptr;
+    ZL_CUDA(cudaMalloc(&d, sizeof(int)));
+    cudaMemset(d, 0, sizeof(int));
+    selftest_wait_kernel<<<1, 64>>>(d, 4096u);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(status, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "selftest");
     return ZLFFT_OK;
 }
 

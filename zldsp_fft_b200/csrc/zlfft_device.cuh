@@ -138,13 +138,50 @@ __device__ __forceinline__ C tw_load(const C* tw, uint32_t t) {
     return tw[t];
 }
 
-// Shared-memory padding: one spare slot per 128 bytes, so that the strided
-// writes of a Stockham exchange fall in distinct banks.
-template <typename C>
-struct SmemPad {
-    static constexpr int kShift = sizeof(C) == 8 ? 4 : 3;  // 16 float2 or 8 double2 per 128 B
-    __device__ __host__ static constexpr uint32_t idx(uint32_t p) { return p + (p >> kShift); }
-    __device__ __host__ static constexpr uint32_t size(uint32_t n) { return n + (n >> kShift) + 1; }
-};
+// ---------------------------------------------------------------- TMA bulk copies
+// 1-D bulk copies global -> shared completed on an mbarrier (sm_90+ PTX,
+// non-multicast). Waits are bounded: after kWaitLimit polls a wait reports
+// failure instead of spinning forever.
+constexpr uint32_t kWaitLimit = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// dst/src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the given phase parity; false if the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kWaitLimit) {
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// Device error word bits (read back by the host with zlfft_plan_device_status).
+constexpr int kDevErrWaitTimeout = 1;
 
 }  // namespace zlfft

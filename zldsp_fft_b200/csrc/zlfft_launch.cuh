@@ -27,7 +27,7 @@ struct TileTable {
 
 template <typename F, int P, int OP, int IL, int OL>
 cudaError_t launch_tile(const TileArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
-    using Cfg = TileCfg<F, P>;
+    using Cfg = TileCfg<F, P, OP>;
     auto kern = tile_kernel<F, P, OP, IL, OL>;
     static const int blocks_per_sm = [kern]() {
         if (Cfg::SMEM > 48 * 1024) {

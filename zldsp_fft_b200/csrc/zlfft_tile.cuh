@@ -4,16 +4,22 @@
 // points in registers and runs the reference's Stockham DIT stages on them:
 // a radix-8 first pass for odd P (src/common/zldsp_fft_common_radix.hpp:477-657),
 // a radix-4 first pass for even P (radix.hpp:170-239), then radix-4 passes
-// with twiddles W_{4L}^{q k} (radix.hpp:78-158, :391-465). Two consecutive
-// radix-4 stages run in registers as one radix-16 group; groups exchange data
-// through padded shared memory in the Stockham (autosort) order, so a
+// with twiddles W_{4L}^{q k} (radix.hpp:78-158, :391-465). Consecutive
+// radix-4 stages run in registers as radix-16 groups; groups exchange data
+// through XOR-swizzled shared memory in the Stockham (autosort) order, so a
 // transform costs one HBM read and one HBM write.
 //
-// The RFFT epilogue/prologue of the reference (execute.hpp:318-368 forward
-// split, :481-536 squared magnitude, :399-451 backward pre-step) is fused: the
-// complex result stays in shared memory and the split runs before the single
-// HBM write (forward), or the pre-step writes shared memory before the first
-// group (backward).
+// Group order: the first (untwiddled) stage group, then a lone radix-4 stage
+// when the count of remaining radix-4 stages is odd, then radix-16 groups.
+// The last group is therefore radix-16 with one butterfly per thread, and
+// its twiddles depend on the thread only: they are loaded into registers
+// once per CTA and reused for every transform the CTA processes.
+//
+// The RFFT epilogue of the reference (execute.hpp:318-368 forward split,
+// :481-536 squared magnitude) is fused after the last group without another
+// shared-memory pass: bins k and N-k live in two adjacent lanes (a mirrored
+// thread order), which exchange them with one warp shuffle. The backward
+// pre-step (execute.hpp:399-451) writes shared memory before the first group.
 //
 // Index algebra (Stockham): after the stages up to sub-length L, element k of
 // sub-transform j sits at position j*L + k. A group of radix R = product of
@@ -44,8 +50,14 @@ struct Grp {
 __host__ __device__ constexpr int tile_num_groups(int P) {
     if (P == 0) return 0;
     if (P == 1) return 1;
-    const int rest = (P % 2) ? (P - 3) / 2 : (P / 2 >= 2 ? P / 2 - 2 : 0);
-    return 1 + rest / 2 + rest % 2;
+    int rest;
+    if (P % 2) {
+        rest = (P - 3) / 2;
+    } else {
+        const int n4 = P / 2;
+        rest = (n4 % 2 == 1) ? n4 - 1 : n4 - 2;
+    }
+    return 1 + rest % 2 + rest / 2;
 }
 
 __host__ __device__ constexpr Grp tile_group(int P, int g) {
@@ -56,24 +68,28 @@ __host__ __device__ constexpr Grp tile_group(int P, int g) {
         g0 = Grp{8, 1, 1, 1};
         rest = (P - 3) / 2;
         L = 8;
-    } else if (P / 2 >= 2) {
+    } else if ((P / 2) % 2 == 1) {
+        g0 = Grp{4, 1, 1, 1};
+        rest = P / 2 - 1;
+        L = 4;
+    } else {
         g0 = Grp{16, 1, 1, 2};
         rest = P / 2 - 2;
         L = 16;
-    } else {
-        g0 = Grp{4, 1, 1, 1};
-        rest = 0;
-        L = 4;
     }
     if (g == 0) return g0;
     int idx = 1;
-    while (rest >= 2) {
-        if (idx == g) return Grp{16, L, 0, 2};
+    if (rest % 2 == 1) {
+        if (g == 1) return Grp{4, L, 0, 1};
+        L *= 4;
+        rest -= 1;
+        idx = 2;
+    }
+    while (idx < g) {
         L *= 16;
-        rest -= 2;
         ++idx;
     }
-    return Grp{4, L, 0, 1};
+    return Grp{16, L, 0, 2};
 }
 
 __host__ __device__ constexpr int tile_elems(int P) {
@@ -100,24 +116,66 @@ struct TileArgs {
     long long in_stride;   // in units of the loaded element (complex; R2C: complex pairs of reals)
     long long out_stride;  // in units of the stored element (complex, or real for sqr_mag)
     const void* tw;        // unified table, 3N/4 complex, N = 2^P
-    const void* rwc;       // RFFT split twiddles 0.5*cos, k = 0..N/2
-    const void* rws;       // RFFT split twiddles 0.5*sin + 0.5
+    const void* tws;       // per-stage tables (see stage_tw_offset), same values as tw
+    const void* rw;        // RFFT split twiddles (0.5*cos, 0.5*sin + 0.5) pairs, k = 0..N/2
+    int* err;              // device error word (kDevErrWaitTimeout on a timed-out wait)
+    int tma;               // inputs qualify for bulk copies (16-byte aligned bases and strides)
 };
 
-template <typename F, int P>
+template <typename F, int P, int OP = kC2CFwd>
 struct TileCfg {
     using C = Cx<F>;
     static constexpr int N = 1 << P;
     static constexpr int E = tile_elems(P);
     static constexpr int T = N / E;  // threads per transform
-    static constexpr int TPC = T >= 256 ? 1 : 256 / T;
+    static constexpr int TPC = T >= 128 ? 1 : 128 / T;
     static constexpr int THREADS = T * TPC;
-    static constexpr int NPAD = (int)SmemPad<C>::size(N);
-    static constexpr size_t SMEM = (size_t)TPC * NPAD * sizeof(C);
+    static constexpr size_t XBYTES = (size_t)TPC * N * sizeof(C);  // exchange buffer
+    // Staging buffer for the next tile's input, filled by TMA bulk copies
+    // while the current tile computes (not for the RFFT backward, whose
+    // pre-step reads the bins directly).
+    static constexpr bool kTMA = P >= 4 && OP != kC2RBwd && 2 * XBYTES <= 200 * 1024;
+    static constexpr size_t SMEM = XBYTES * (kTMA ? 2 : 1) + (kTMA ? 16 : 0);
     static constexpr int NG = tile_num_groups(P);
-    // Register budget: enough resident CTAs for ~80 registers per thread.
-    static constexpr int MINB = (65536 / (THREADS * 80)) > 0 ? (65536 / (THREADS * 80)) : 1;
+    // Register budget: enough resident CTAs for ~96 registers per thread in
+    // FP32 (the last group's 15 complex twiddles stay in registers), ~128 in FP64.
+    static constexpr int REGS = sizeof(F) == 4 ? 96 : 128;
+    static constexpr int MINB = (65536 / (THREADS * REGS)) > 0 ? (65536 / (THREADS * REGS)) : 1;
 };
+
+// XOR swizzle of a shared-memory slot index: keeps each 128-byte row, permutes
+// the slots inside it so the strided Stockham writes and the unit-stride reads
+// hit distinct banks (checked by simulation for every exchange of every order).
+template <typename C>
+__device__ __forceinline__ uint32_t swz(uint32_t p) {
+    if constexpr (sizeof(C) == 8) {
+        return p ^ (((p >> 4) ^ (p >> 7)) & 15u);
+    } else {
+        return p ^ (((p >> 3) + (p >> 6)) & 7u);
+    }
+}
+
+// Swizzle of the exchange that feeds a mirrored last group (RFFT forward): its
+// reads are two runs of 16 consecutive slots, one of them offset by one slot
+// from a 128-byte row, so only the writer's run blocks (LW consecutive slots,
+// LW rows apart) are separated, by XOR of whole LW-slot blocks. Checked by
+// simulation to be conflict-free for the orders that use it (8, 10, 11, 12, 14).
+template <typename C, int LW>
+__device__ __forceinline__ uint32_t swz_mirror(uint32_t p) {
+    if constexpr (sizeof(C) != 8 || LW >= 16) {
+        return sizeof(C) == 8 ? p : swz<C>(p);
+    } else {
+        const uint32_t r = p >> 4;
+        return p ^ (((r / LW) & (16u / LW - 1u)) * LW);
+    }
+}
+
+// Per-stage twiddle tables: the radix-4 stage with sub-length L (twiddles
+// W_{4L}^{qk}, q = 1..3, k < L) occupies 3L consecutive entries at offset
+// L - L0, q-major, where L0 is the first twiddled stage's sub-length (4 for
+// even orders, 8 for odd). Threads with consecutive k read consecutive
+// entries. The values are copies of the unified table's entries.
+__host__ __device__ constexpr int stage_l0(int P) { return (P % 2) ? 8 : 4; }
 
 // ---------------------------------------------------------------- global I/O
 // A complex stream seen from one transform's base: AoS is one array of
@@ -169,11 +227,44 @@ struct CxOut {
 };
 
 // ---------------------------------------------------------------- group compute
-// Runs the stages of a group (R points, entry sub-length L) on the R
-// registers r[] of one butterfly with in-group index k (k < L).
-// Output register s then holds output mu(s) (see group_mu).
+// Twiddles of a group for in-group index k: radix-4 non-first: w[0..2] =
+// W_{4L}^{qk}; radix-16 non-first: w[0..2] (stage A) then w[3+3m+(q-1)] =
+// W_{16L}^{q(k+mL)} (stage B, m = 0..3); radix-16 first: stage B only.
+template <int P, int R, int L, int FIRST>
+__host__ __device__ constexpr int group_tw_count() {
+    return R == 4 ? (FIRST ? 0 : 3) : R == 16 ? (FIRST ? 12 : 15) : 0;
+}
+
 template <int P, int R, int L, int FIRST, typename C>
-__device__ __forceinline__ void group_compute(C* r, uint32_t k, const C* tw) {
+__device__ __forceinline__ void group_load_tw(const C* tw, uint32_t k, C* w) {
+    if constexpr (R == 4 && !FIRST) {
+        constexpr int s = P - ilog2c(4LL * L);
+        w[0] = tw_load(tw, (1u * k) << s);
+        w[1] = tw_load(tw, (2u * k) << s);
+        w[2] = tw_load(tw, (3u * k) << s);
+    } else if constexpr (R == 16) {
+        constexpr int o = FIRST ? 0 : 3;
+        if constexpr (!FIRST) {
+            constexpr int s = P - ilog2c(4LL * L);
+            w[0] = tw_load(tw, (1u * k) << s);
+            w[1] = tw_load(tw, (2u * k) << s);
+            w[2] = tw_load(tw, (3u * k) << s);
+        }
+        constexpr int s2 = P - ilog2c(16LL * L);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const uint32_t kk = k + (uint32_t)(m * L);
+            w[o + 3 * m + 0] = tw_load(tw, (1u * kk) << s2);
+            w[o + 3 * m + 1] = tw_load(tw, (2u * kk) << s2);
+            w[o + 3 * m + 2] = tw_load(tw, (3u * kk) << s2);
+        }
+    }
+}
+
+// Runs the stages of a group on the R registers r[] of one butterfly.
+// Output register s then holds output mu(s) (see group_mu).
+template <int R, int FIRST, typename C>
+__device__ __forceinline__ void group_compute(C* r, const C* w) {
     if constexpr (R == 2) {
         bfly2(r[0], r[1]);
     } else if constexpr (R == 8) {
@@ -182,28 +273,51 @@ __device__ __forceinline__ void group_compute(C* r, uint32_t k, const C* tw) {
         if constexpr (FIRST) {
             bfly4_first(r[0], r[1], r[2], r[3]);
         } else {
-            constexpr int s = P - ilog2c(4LL * L);
-            const C w1 = tw_load(tw, (1u * k) << s), w2 = tw_load(tw, (2u * k) << s), w3 = tw_load(tw, (3u * k) << s);
-            bfly4_tw(r[0], r[1], r[2], r[3], w1, w2, w3);
+            bfly4_tw(r[0], r[1], r[2], r[3], w[0], w[1], w[2]);
         }
     } else {  // R == 16: two radix-4 stages
+        constexpr int o = FIRST ? 0 : 3;
         if constexpr (FIRST) {
 #pragma unroll
             for (int a = 0; a < 4; ++a) bfly4_first(r[a], r[a + 4], r[a + 8], r[a + 12]);
         } else {
-            constexpr int s = P - ilog2c(4LL * L);
-            const C w1 = tw_load(tw, (1u * k) << s), w2 = tw_load(tw, (2u * k) << s), w3 = tw_load(tw, (3u * k) << s);
+#pragma unroll
+            for (int a = 0; a < 4; ++a) bfly4_tw(r[a], r[a + 4], r[a + 8], r[a + 12], w[0], w[1], w[2]);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+            bfly4_tw(r[4 * m], r[4 * m + 1], r[4 * m + 2], r[4 * m + 3], w[o + 3 * m], w[o + 3 * m + 1],
+                     w[o + 3 * m + 2]);
+    }
+}
+
+// As group_compute, loading each butterfly's twiddles from the table right
+// before use (short live ranges; used where the twiddles are not held in
+// registers across transforms).
+template <int P, int R, int L, int FIRST, typename C>
+__device__ __forceinline__ void group_compute_ld(C* r, uint32_t k, const C* tws) {
+    constexpr int L0 = stage_l0(P);
+    if constexpr (R == 4 && !FIRST) {
+        const C* t = tws + (L - L0) + k;
+        bfly4_tw(r[0], r[1], r[2], r[3], tw_load(t, 0), tw_load(t, L), tw_load(t, 2 * L));
+    } else if constexpr (R == 16) {
+        if constexpr (FIRST) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) bfly4_first(r[a], r[a + 4], r[a + 8], r[a + 12]);
+        } else {
+            const C* t = tws + (L - L0) + k;
+            const C w1 = tw_load(t, 0), w2 = tw_load(t, L), w3 = tw_load(t, 2 * L);
 #pragma unroll
             for (int a = 0; a < 4; ++a) bfly4_tw(r[a], r[a + 4], r[a + 8], r[a + 12], w1, w2, w3);
         }
-        constexpr int s2 = P - ilog2c(16LL * L);
+        const C* t2 = tws + (4 * L - L0) + k;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            const uint32_t kk = k + (uint32_t)(m * L);
-            const C w1 = tw_load(tw, (1u * kk) << s2), w2 = tw_load(tw, (2u * kk) << s2),
-                    w3 = tw_load(tw, (3u * kk) << s2);
-            bfly4_tw(r[4 * m], r[4 * m + 1], r[4 * m + 2], r[4 * m + 3], w1, w2, w3);
+            bfly4_tw(r[4 * m], r[4 * m + 1], r[4 * m + 2], r[4 * m + 3], tw_load(t2, m * L),
+                     tw_load(t2, m * L + 4 * L), tw_load(t2, m * L + 8 * L));
         }
+    } else {
+        group_compute<R, FIRST>(r, (const C*)nullptr);
     }
 }
 
@@ -212,23 +326,116 @@ __host__ __device__ constexpr int group_mu(const Grp G, int s) {
     return G.nst == 2 ? (s >> 2) + 4 * (s & 3) : s;
 }
 
+// Butterfly of thread lt in a last group with one butterfly per thread and
+// L = T butterflies. With MIRROR, threads come in groups of 2H (H = half a
+// warp, or T/2 when T < 32): the lower H threads hold b = j, the upper H hold
+// b = L - j for the same j (b = L/2 for j = 0), so bins k and N - k sit in
+// lanes that differ by H. Each half-warp still reads consecutive positions.
+template <bool MIRROR, int T>
+__device__ __forceinline__ int last_butterfly(int lt, int L) {
+    if constexpr (!MIRROR) {
+        return lt;
+    } else {
+        constexpr int H = (T < 32 ? T : 32) / 2;
+        const int g = lt / (2 * H), l = lt % (2 * H);
+        const int j = g * H + (l % H);
+        return l < H ? j : (j == 0 ? L / 2 : L - j);
+    }
+}
+
+// The RFFT forward split of one bin pair from z1 = Z[k], z2 = Z[N-k]
+// (src/common/zldsp_fft_common_execute.hpp:347-358).
+template <typename F>
+struct SplitOut {
+    F xr_k, xi_k, xr_m, xi_m;
+};
+template <typename F, typename C>
+__device__ __forceinline__ SplitOut<F> rfft_split(C z1, C z2, F c, F s) {
+    const F si = z1.y + z2.y, dr = z1.x - z2.x;
+    SplitOut<F> o;
+    o.xr_k = fma_rn(-dr, s, fma_rn(si, c, z1.x));
+    o.xi_k = fma_rn(-dr, c, fma_rn(-si, s, z1.y));
+    o.xr_m = fma_rn(dr, s, fma_rn(-si, c, z2.x));
+    o.xi_m = fma_rn(-dr, c, fma_rn(-si, s, z2.y));
+    return o;
+}
+
 // ---------------------------------------------------------------- the kernel
 template <typename F, int P, int OP, int IL, int OL>
-__global__ void __launch_bounds__(TileCfg<F, P>::THREADS, TileCfg<F, P>::MINB) tile_kernel(const TileArgs a) {
-    using Cfg = TileCfg<F, P>;
+__global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>::MINB) tile_kernel(const TileArgs a) {
+    using Cfg = TileCfg<F, P, OP>;
     using C = Cx<F>;
-    using Pad = SmemPad<C>;
     constexpr int N = Cfg::N, E = Cfg::E, T = Cfg::T, TPC = Cfg::TPC, NG = Cfg::NG;
     constexpr bool kFwd = (OP == kC2CFwd || OP == kR2CFwd || OP == kR2CSqrMag);
     constexpr bool kR2C = (OP == kR2CFwd || OP == kR2CSqrMag);
+    constexpr Grp GL = tile_group(P, NG > 0 ? NG - 1 : 0);
+    // last group: one butterfly per thread, twiddles held in registers (FP32;
+    // FP64 twiddles would take twice the registers and are read from L1)
+    constexpr bool kLastReg = NG >= 2 && GL.R == E && !GL.first && sizeof(F) == 4;
+    constexpr bool kShufPost = kR2C && NG >= 2 && GL.R == E && !GL.first && GL.R == 16 && T >= 2;
+    constexpr int kLastTw = group_tw_count<P, GL.R, GL.L, GL.first>();
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw);
     const int lt = (int)threadIdx.x % T;
     const int slot = (int)threadIdx.x / T;
-    C* sx = reinterpret_cast<C*>(smem_raw) + (size_t)slot * Cfg::NPAD;
+    const uint32_t sbase = (uint32_t)slot * N;
+    auto sidx = [&](int pos) -> uint32_t { return swz<C>(sbase + (uint32_t)pos); };
     const C* tw = static_cast<const C*>(a.tw);
+    const C* tws = static_cast<const C*>(a.tws);
+
+    const int b_last = last_butterfly<kShufPost, T>(lt, GL.L);
+    constexpr int H = (T < 32 ? T : 32) / 2;  // partner-lane distance of the shuffle split
+    C wl[kLastTw > 0 ? kLastTw : 1];
+    if constexpr (kLastReg) group_load_tw<P, GL.R, GL.L, GL.first>(tw, (uint32_t)(b_last % GL.L), wl);
+
+    // ---- TMA staging of each tile's input (one tile ahead)
+    constexpr bool kSoAIn = (IL == kSoA) && !kR2C;
+    C* stage = sm + (size_t)TPC * N;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::XBYTES * 2);
+    const bool use_tma = Cfg::kTMA && a.tma;
+    auto issue = [&](long long t) {  // warp 0 issues the copies of tile t
+        if (!use_tma || threadIdx.x >= 32 || t * TPC >= a.batch) return;
+        const long long left = a.batch - t * TPC;
+        const int nvalid = (int)(left < TPC ? left : TPC);
+        constexpr uint32_t kSlot = (uint32_t)(N * sizeof(C));
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, kSlot * (uint32_t)nvalid);
+        __syncwarp();
+        for (int q = (int)threadIdx.x; q < nvalid; q += 32) {
+            const long long base = (t * TPC + q) * a.in_stride;
+            if constexpr (kSoAIn) {
+                F* dst = reinterpret_cast<F*>(stage + (size_t)q * N);
+                bulk_g2s(dst, static_cast<const F*>(a.in0) + base, kSlot / 2, bar);
+                bulk_g2s(dst + N, static_cast<const F*>(a.in1) + base, kSlot / 2, bar);
+            } else {
+                bulk_g2s(stage + (size_t)q * N, static_cast<const C*>(a.in0) + base, kSlot, bar);
+            }
+        }
+    };
+    if constexpr (Cfg::kTMA) {
+        if (use_tma) {
+            if (threadIdx.x == 0) {
+                mbar_init(bar, 1);
+                fence_mbar_init();
+            }
+            __syncthreads();
+            issue(blockIdx.x);
+        }
+    }
+    uint32_t phase = 0;
 
     for (long long tile = blockIdx.x; tile * TPC < a.batch; tile += gridDim.x) {
+        if constexpr (Cfg::kTMA) {
+            if (use_tma) {
+                const bool ok = mbar_wait(bar, phase);
+                if (__syncthreads_or(!ok)) {  // bounded wait ran out: report and leave
+                    if (threadIdx.x == 0) atomicOr(a.err, kDevErrWaitTimeout);
+                    mbar_wait(bar, phase);  // give copies in flight a bounded chance to land
+                    return;
+                }
+                phase ^= 1u;
+            }
+        }
         const long long tr = tile * TPC + slot;
         const bool valid = tr < a.batch;
         const long long ibase = valid ? tr * a.in_stride : 0;
@@ -239,109 +446,193 @@ __global__ void __launch_bounds__(TileCfg<F, P>::THREADS, TileCfg<F, P>::MINB) t
         if constexpr (OP == kC2RBwd) {
             // Backward RFFT pre-step into shared memory (execute.hpp:399-451).
             if (valid) {
-                const F* rwc = static_cast<const F*>(a.rwc);
-                const F* rws = static_cast<const F*>(a.rws);
+                const C* rw = static_cast<const C*>(a.rw);
                 const CxIn<F, IL> in(a.in0, a.in1, ibase);
                 for (int k = 1 + lt; k <= N / 2; k += T) {
                     const C x1 = in[k];
                     const C x2 = in[N - k];
-                    const F c = rwc[k], s = rws[k];
+                    const C w = rw[k];
+                    const F c = w.x, s = w.y;
                     const F si = x1.y + x2.y, dr = x1.x - x2.x;
                     const C zk = cx<C>(fma_rn(-dr, s, fma_rn(-si, c, x1.x)), fma_rn(dr, c, fma_rn(-si, s, x1.y)));
                     const C zm = cx<C>(fma_rn(dr, s, fma_rn(si, c, x2.x)), fma_rn(dr, c, fma_rn(-si, s, x2.y)));
-                    if (k != N / 2) sx[Pad::idx(k)] = zk;
-                    sx[Pad::idx(N - k)] = zm;
+                    if (k != N / 2) sm[sidx(k)] = zk;
+                    sm[sidx(N - k)] = zm;
                 }
                 if (lt == 0) {
                     const C x0 = in[0];
                     const C xm = in[N];
-                    sx[0] = cx<C>(mul_rn(x0.x + xm.x, (F)0.5), mul_rn(x0.x - xm.x, (F)0.5));
+                    sm[sidx(0)] = cx<C>(mul_rn(x0.x + xm.x, (F)0.5), mul_rn(x0.x - xm.x, (F)0.5));
                 }
             }
             __syncthreads();
-            if constexpr (NG > 0) {
-                constexpr Grp G0 = tile_group(P, 0);
-#pragma unroll
-                for (int u = 0; u < E / G0.R; ++u) {
-                    const int b = lt + u * T;
-#pragma unroll
-                    for (int rho = 0; rho < G0.R; ++rho) v[u * G0.R + rho] = cswap(sx[Pad::idx(b + rho * (N / G0.R))]);
-                }
-            } else {
-                v[0] = cswap(sx[0]);
-            }
-        } else {
-            constexpr int IL2 = kR2C ? (int)kAoS : IL;
-            const CxIn<F, IL2> in(a.in0, a.in1, ibase);
-            if constexpr (NG > 0) {
-                constexpr Grp G0 = tile_group(P, 0);
-#pragma unroll
-                for (int u = 0; u < E / G0.R; ++u) {
-                    const int b = lt + u * T;
-#pragma unroll
-                    for (int rho = 0; rho < G0.R; ++rho) {
-                        C x = valid ? in[b + rho * (N / G0.R)] : cx<C>((F)0, (F)0);
-                        v[u * G0.R + rho] = kFwd ? x : cswap(x);
-                    }
-                }
-            } else {
-                C x = valid ? in[0] : cx<C>((F)0, (F)0);
-                v[0] = kFwd ? x : cswap(x);
-            }
         }
 
         // ------------------------------------------------ stage groups
-        // Final complex results go to global memory (C2C, C2R) or, for the
-        // forward RFFT, to shared memory for the split epilogue.
         constexpr int OL2 = (OP == kC2RBwd || OP == kR2CSqrMag) ? (int)kAoS : OL;
         const CxOut<F, OL2> out(a.out0, a.out1, obase);
-        auto emit = [&](int pos, C val) {
-            if constexpr (kR2C) {
-                sx[Pad::idx(pos)] = val;
-            } else {
-                if (valid) out.put(pos, kFwd ? val : cswap(val));
-            }
-        };
         if constexpr (NG == 0) {
-            emit(0, v[0]);
+            C x;
+            if constexpr (OP == kC2RBwd) {
+                x = cswap(sm[sidx(0)]);
+            } else {
+                constexpr int IL2 = kR2C ? (int)kAoS : IL;
+                const CxIn<F, IL2> in(a.in0, a.in1, ibase);
+                x = valid ? in[0] : cx<C>((F)0, (F)0);
+                if constexpr (!kFwd) x = cswap(x);
+            }
+            v[0] = x;
+            if constexpr (kR2C) {
+                sm[sidx(0)] = v[0];
+            } else if (valid) {
+                out.put(0, kFwd ? v[0] : cswap(v[0]));
+            }
         } else {
-            // Unrolled over groups through a constexpr index sequence.
             [&]<int... GI>(std::integer_sequence<int, GI...>) {
                 (
                     [&] {
                         constexpr Grp G = tile_group(P, GI);
                         constexpr int NB = E / G.R;
-                        if constexpr (GI > 0) {
-                            // Read this group's inputs from the exchange buffer.
+                        constexpr bool kLast = (GI + 1 == NG);
+                        // ---- inputs of this group
+                        if constexpr (GI == 0 && OP != kC2RBwd) {
+                            if (use_tma) {
+                                const C* sc = stage + (size_t)slot * N;
+                                const F* sf = reinterpret_cast<const F*>(sc);
+#pragma unroll
+                                for (int u = 0; u < NB; ++u) {
+                                    const int b = (kLast ? b_last : lt) + u * T;
+#pragma unroll
+                                    for (int rho = 0; rho < G.R; ++rho) {
+                                        const int pos = b + rho * (N / G.R);
+                                        C x = kSoAIn ? cx<C>(sf[pos], sf[N + pos]) : sc[pos];
+                                        v[u * G.R + rho] = kFwd ? x : cswap(x);
+                                    }
+                                }
+                                __syncthreads();  // staging fully read: refill it with the next tile
+                                issue(tile + gridDim.x);
+                            } else {
+                                constexpr int IL2 = kR2C ? (int)kAoS : IL;
+                                const CxIn<F, IL2> in(a.in0, a.in1, ibase);
+#pragma unroll
+                                for (int u = 0; u < NB; ++u) {
+                                    const int b = (kLast ? b_last : lt) + u * T;
+#pragma unroll
+                                    for (int rho = 0; rho < G.R; ++rho) {
+                                        C x = valid ? in[b + rho * (N / G.R)] : cx<C>((F)0, (F)0);
+                                        v[u * G.R + rho] = kFwd ? x : cswap(x);
+                                    }
+                                }
+                            }
+                        } else {
 #pragma unroll
                             for (int u = 0; u < NB; ++u) {
-                                const int b = lt + u * T;
+                                const int b = (kLast ? b_last : lt) + u * T;
 #pragma unroll
-                                for (int rho = 0; rho < G.R; ++rho) v[u * G.R + rho] = sx[Pad::idx(b + rho * (N / G.R))];
+                                for (int rho = 0; rho < G.R; ++rho) {
+                                    const int pos = b + rho * (N / G.R);
+                                    uint32_t ix;
+                                    if constexpr (kShufPost && kLast) {
+                                        ix = swz_mirror<C, tile_group(P, NG >= 2 ? NG - 2 : 0).L>(sbase + (uint32_t)pos);
+                                    } else {
+                                        ix = sidx(pos);
+                                    }
+                                    const C x = sm[ix];
+                                    v[u * G.R + rho] = (GI == 0 && OP == kC2RBwd) ? cswap(x) : x;
+                                }
                             }
                         }
+                        // ---- compute
+                        if constexpr (kLast && kLastReg) {
+                            group_compute<G.R, G.first>(v, wl);
+                        } else {
 #pragma unroll
-                        for (int u = 0; u < NB; ++u) {
-                            const int b = lt + u * T;
-                            group_compute<P, G.R, G.L, G.first>(v + u * G.R, (uint32_t)(b % G.L), tw);
+                            for (int u = 0; u < NB; ++u) {
+                                const int b = (kLast ? b_last : lt) + u * T;
+                                group_compute_ld<P, G.R, G.L, G.first>(v + u * G.R, (uint32_t)(b % G.L), tws);
+                            }
                         }
-                        if constexpr (GI + 1 < NG) {
+                        // ---- outputs
+                        if constexpr (!kLast) {
                             __syncthreads();
 #pragma unroll
                             for (int u = 0; u < NB; ++u) {
                                 const int b = lt + u * T;
                                 const int J = b / G.L, k = b % G.L;
 #pragma unroll
-                                for (int s = 0; s < G.R; ++s)
-                                    sx[Pad::idx(J * G.R * G.L + k + group_mu(G, s) * G.L)] = v[u * G.R + s];
+                                for (int s = 0; s < G.R; ++s) {
+                                    const int pos = J * G.R * G.L + k + group_mu(G, s) * G.L;
+                                    uint32_t ix;
+                                    if constexpr (kShufPost && GI + 2 == NG) {
+                                        ix = swz_mirror<C, G.L>(sbase + (uint32_t)pos);
+                                    } else {
+                                        ix = sidx(pos);
+                                    }
+                                    sm[ix] = v[u * G.R + s];
+                                }
                             }
                             __syncthreads();
+                        } else if constexpr (kShufPost) {
+                            // RFFT split from registers: z[mu] = Z[b + mu*L]; the partner lane
+                            // (lt ^ H) holds Z[N - b - mu*L] at slot 15 - mu (for the lanes
+                            // holding b = 0 and b = L/2 the partner is the lane itself).
+                            constexpr int L = G.L;
+                            C z[16];
+#pragma unroll
+                            for (int s = 0; s < 16; ++s) z[group_mu(G, s)] = v[s];
+                            const C* rw = static_cast<const C*>(a.rw);
+                            [[maybe_unused]] F* osq = static_cast<F*>(a.out0) + obase;
+#pragma unroll
+                            for (int m = 0; m < 8; ++m) {
+                                C p;
+                                p.x = __shfl_xor_sync(0xffffffffu, z[15 - m].x, H);
+                                p.y = __shfl_xor_sync(0xffffffffu, z[15 - m].y, H);
+                                C z2 = p;
+                                const int k = b_last + m * L;
+                                if (lt == 0) {  // b = 0: pairs (m, 16 - m); m = 0 is DC/Nyquist
+                                    z2 = z[(16 - m) & 15];
+                                } else if (lt == H) {  // b = L/2: pairs (m, 15 - m) in this lane
+                                    z2 = z[15 - m];
+                                }
+                                if (valid && !(lt == 0 && m == 0)) {
+                                    const C w = rw[k];
+                                    const SplitOut<F> o = rfft_split<F>(z[m], z2, w.x, w.y);
+                                    if constexpr (OP == kR2CFwd) {
+                                        if (k != N / 2) out.put(k, cx<C>(o.xr_k, o.xi_k));
+                                        out.put(N - k, cx<C>(o.xr_m, o.xi_m));
+                                    } else {
+                                        if (k != N / 2) __stcs(osq + k, fma_rn(o.xr_k, o.xr_k, mul_rn(o.xi_k, o.xi_k)));
+                                        __stcs(osq + N - k, fma_rn(o.xr_m, o.xr_m, mul_rn(o.xi_m, o.xi_m)));
+                                    }
+                                }
+                            }
+                            if (valid && lt == 0) {  // b = 0 also owns k = N/2 (slot 8) and DC/Nyquist
+                                const C w = rw[N / 2];
+                                const SplitOut<F> o = rfft_split<F>(z[8], z[8], w.x, w.y);
+                                const F dc = z[0].x + z[0].y, ny = z[0].x - z[0].y;
+                                if constexpr (OP == kR2CFwd) {
+                                    out.put(N / 2, cx<C>(o.xr_m, o.xi_m));
+                                    out.put(0, cx<C>(dc, (F)0));
+                                    out.put(N, cx<C>(ny, (F)0));
+                                } else {
+                                    __stcs(osq + N / 2, fma_rn(o.xr_m, o.xr_m, mul_rn(o.xi_m, o.xi_m)));
+                                    __stcs(osq, mul_rn(dc, dc));
+                                    __stcs(osq + N, mul_rn(ny, ny));
+                                }
+                            }
                         } else {
 #pragma unroll
                             for (int u = 0; u < NB; ++u) {
-                                const int b = lt + u * T;  // J == 0 in the last group
+                                const int b = b_last + u * T;  // J == 0 in the last group
 #pragma unroll
-                                for (int s = 0; s < G.R; ++s) emit(b + group_mu(G, s) * G.L, v[u * G.R + s]);
+                                for (int s = 0; s < G.R; ++s) {
+                                    const int pos = b + group_mu(G, s) * G.L;
+                                    if constexpr (kR2C) {
+                                        sm[sidx(pos)] = v[u * G.R + s];
+                                    } else if (valid) {
+                                        out.put(pos, kFwd ? v[u * G.R + s] : cswap(v[u * G.R + s]));
+                                    }
+                                }
                             }
                         }
                     }(),
@@ -349,44 +640,40 @@ __global__ void __launch_bounds__(TileCfg<F, P>::THREADS, TileCfg<F, P>::MINB) t
             }(std::make_integer_sequence<int, NG>{});
         }
 
-        // ------------------------------------------------ RFFT forward split
-        if constexpr (kR2C) {
+        // ------------------------------------------------ RFFT forward split through shared memory
+        // (orders without a shuffle-friendly last group)
+        if constexpr (kR2C && !kShufPost) {
             __syncthreads();
             if (valid) {
-                const F* rwc = static_cast<const F*>(a.rwc);
-                const F* rws = static_cast<const F*>(a.rws);
+                const C* rw = static_cast<const C*>(a.rw);
+                [[maybe_unused]] F* osq = static_cast<F*>(a.out0) + obase;
                 for (int k = 1 + lt; k <= N / 2; k += T) {
-                    const C z1 = sx[Pad::idx(k)], z2 = sx[Pad::idx(N - k)];
-                    const F c = rwc[k], s = rws[k];
-                    const F si = z1.y + z2.y, dr = z1.x - z2.x;
-                    const F xr_k = fma_rn(-dr, s, fma_rn(si, c, z1.x));
-                    const F xi_k = fma_rn(-dr, c, fma_rn(-si, s, z1.y));
-                    const F xr_m = fma_rn(dr, s, fma_rn(-si, c, z2.x));
-                    const F xi_m = fma_rn(-dr, c, fma_rn(-si, s, z2.y));
+                    const C w = rw[k];
+                    const SplitOut<F> o = rfft_split<F>(sm[sidx(k)], sm[sidx(N - k)], w.x, w.y);
                     if constexpr (OP == kR2CFwd) {
-                        if (k != N / 2) out.put(k, cx<C>(xr_k, xi_k));
-                        out.put(N - k, cx<C>(xr_m, xi_m));
+                        if (k != N / 2) out.put(k, cx<C>(o.xr_k, o.xi_k));
+                        out.put(N - k, cx<C>(o.xr_m, o.xi_m));
                     } else {
-                        F* o = static_cast<F*>(a.out0) + obase;
-                        if (k != N / 2) __stcs(o + k, fma_rn(xr_k, xr_k, mul_rn(xi_k, xi_k)));
-                        __stcs(o + N - k, fma_rn(xr_m, xr_m, mul_rn(xi_m, xi_m)));
+                        if (k != N / 2) __stcs(osq + k, fma_rn(o.xr_k, o.xr_k, mul_rn(o.xi_k, o.xi_k)));
+                        __stcs(osq + N - k, fma_rn(o.xr_m, o.xr_m, mul_rn(o.xi_m, o.xi_m)));
                     }
                 }
                 if (lt == 0) {
-                    const C z0 = sx[0];
+                    const C z0 = sm[sidx(0)];
                     const F dc = z0.x + z0.y, ny = z0.x - z0.y;
                     if constexpr (OP == kR2CFwd) {
                         out.put(0, cx<C>(dc, (F)0));
                         out.put(N, cx<C>(ny, (F)0));
                     } else {
-                        F* o = static_cast<F*>(a.out0) + obase;
-                        __stcs(o, mul_rn(dc, dc));
-                        __stcs(o + N, mul_rn(ny, ny));
+                        __stcs(osq, mul_rn(dc, dc));
+                        __stcs(osq + N, mul_rn(ny, ny));
                     }
                 }
             }
         }
-        __syncthreads();  // the exchange buffer is reused by the next tile
+        // The next tile's first shared-memory write is preceded by a barrier in
+        // every path except the backward RFFT pre-step and the single-point case.
+        if constexpr (OP == kC2RBwd || NG == 0) __syncthreads();
     }
 }
 

@@ -88,6 +88,12 @@ class Plan:
         C.check(self._lib.zlfft_plan_take_launch_count(self.handle, ctypes.byref(v)))
         return v.value
 
+    def device_status(self) -> int:
+        """Synchronise, then read and clear the plan's device error word (0 = ok)."""
+        v = ctypes.c_int()
+        self._lib.zlfft_plan_device_status(self.handle, ctypes.byref(v))
+        return v.value
+
     def twiddles(self) -> np.ndarray:
         """The device-generated unified twiddle table, copied to the host."""
         n = ctypes.c_size_t()
