@@ -249,3 +249,79 @@ def test_bounded_wait_reports_instead_of_hanging():
     x = np.ones((2, 256), np.complex64)
     y = G.run_c2c(plan, x, True)
     assert y[0, 0] == 256
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+@pytest.mark.parametrize("order", [14, 15, 16, 17, 18, 19, 20])
+def test_multipass_cfft(oracle, prec, ft, ct, order):
+    """Orders above one CTA: 2-3 Stockham passes through L2-resident scratch;
+    the arithmetic is still the reference's, so f32 stays bit-exact."""
+    n = 1 << order
+    rng = np.random.default_rng(3000 + order)
+    b = 2
+    x = _cx(rng, b, n, ct)
+    plan = Z.Plan(Z.C2C, order, ft)
+    tol = oracle.tolerance(order, prec)
+    layouts = [(Z.AOS, Z.AOS), (Z.SOA, Z.SOA)] if order > 16 else [(i, o) for i in (Z.AOS, Z.SOA) for o in (Z.AOS, Z.SOA)]
+    for forward in (True, False):
+        port = oracle.cfft_port(x, forward)
+        fp64 = oracle.cfft_fp64(x, forward)
+        for il, ol in layouts:
+            y = G.run_c2c(plan, x, forward, il, ol)
+            assert oracle.rel_l2(y, fp64).max() <= tol, (order, forward, il, ol)
+            if prec == "f32":
+                assert np.array_equal(y, port), (order, forward, il, ol)
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+@pytest.mark.parametrize("order", [15, 16, 17])
+def test_multipass_rfft(oracle, prec, ft, ct, order):
+    n = 1 << order
+    rng = np.random.default_rng(4000 + order)
+    x = rng.uniform(-1, 1, (2, n)).astype(ft)
+    plan = Z.Plan(Z.R2C, order, ft)
+    tol = oracle.tolerance(order, prec)
+    for ol in (Z.AOS, Z.SOA):
+        X = G.run_r2c(plan, x, ol)
+        assert oracle.rel_l2(X, oracle.rfft_fp64(x)).max() <= tol
+        if prec == "f32":
+            assert np.array_equal(X, oracle.rfft_forward_port(x)), (order, ol)
+    P = G.run_r2c(plan, x, sqr_mag=True)
+    if prec == "f32":
+        assert np.array_equal(P, oracle.rfft_forward_port(x, sqr_mag=True))
+    Xin = _cx(rng, 2, n // 2 + 1, ct)
+    for il in (Z.AOS, Z.SOA):
+        back = G.run_c2r(plan, Xin, il)
+        assert oracle.rel_l2(back, oracle.rfft_backward_fp64(Xin)).max() <= tol
+        if prec == "f32":
+            assert np.array_equal(back, oracle.rfft_backward_port(Xin)), (order, il)
+
+
+def test_multipass_chunks_strides_inplace(oracle):
+    """More transforms than one scratch chunk, ragged strides, and in place."""
+    import torch
+    order, n = 16, 1 << 16
+    plan = Z.Plan(Z.C2C, order, np.float32)
+    rng = np.random.default_rng(11)
+    b = 100  # chunks hold 48 transforms of 2^16 complex f32
+    x = (rng.uniform(-1, 1, (b, n)) + 1j * rng.uniform(-1, 1, (b, n))).astype(np.complex64)
+    y = G.run_c2c(plan, x, True)
+    idx = [0, 47, 48, 99]
+    assert np.array_equal(y[idx], oracle.cfft_port(x[idx], True))
+    t = G.dev(x)
+    plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, t.data_ptr(), None, t.data_ptr(), None, b)
+    torch.cuda.synchronize()
+    assert np.array_equal(G.host(t)[idx], y[idx])
+    si, so = n + 24, n + 8
+    buf = np.zeros(3 * si, np.complex64)
+    for i in range(3):
+        buf[i * si: i * si + n] = x[i]
+    ti = G.dev(buf)
+    to = torch.zeros((3 * so, 2), dtype=torch.float32, device="cuda")
+    plan.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, ti.data_ptr(), None, to.data_ptr(), None, 3, si, so)
+    torch.cuda.synchronize()
+    o = G.host(to)
+    o = (o[:, 0] + 1j * o[:, 1]).astype(np.complex64)
+    ref = oracle.cfft_port(x[:3], False)
+    for i in range(3):
+        assert np.array_equal(o[i * so: i * so + n], ref[i])

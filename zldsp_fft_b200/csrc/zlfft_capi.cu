@@ -9,6 +9,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 
@@ -111,11 +112,17 @@ __global__ void selftest_wait_kernel(int* err, uint32_t limit) {
 struct TablesHolder {
     zlfft::TileTable f32{};
     zlfft::TileTable f64{};
+    zlfft::PassTable p32{};
+    zlfft::PassTable p64{};
     TablesHolder() {
         zlfft::fill_tile_c2c_f32(f32);
         zlfft::fill_tile_r2c_f32(f32);
         zlfft::fill_tile_c2c_f64(f64);
         zlfft::fill_tile_r2c_f64(f64);
+        zlfft::fill_pass_f32_a(p32);
+        zlfft::fill_pass_f32_b(p32);
+        zlfft::fill_pass_f64_a(p64);
+        zlfft::fill_pass_f64_b(p64);
     }
 };
 
@@ -148,6 +155,10 @@ struct zlfft_plan_s {
     void* d_out = nullptr;
     size_t stage_in_bytes = 0, stage_out_bytes = 0;
     size_t launches = 0;
+    // multi-pass scratch (two buffers of `chunk` transforms each)
+    void* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    size_t chunk = 0;  // transforms per chunk; intermediates of one chunk stay L2-resident
     int* d_err = nullptr;  // device error word written by kernels (bounded waits that ran out)
     std::mutex mu;
 };
@@ -172,6 +183,7 @@ void release(zlfft_plan p) {
     if (p->d_tws) cudaFree(p->d_tws);
     if (p->d_rw) cudaFree(p->d_rw);
     if (p->d_err) cudaFree(p->d_err);
+    if (p->d_scratch) cudaFree(p->d_scratch);
     if (p->d_in) cudaFree(p->d_in);
     if (p->d_out) cudaFree(p->d_out);
     if (p->h_in) cudaFreeHost(p->h_in);
@@ -213,6 +225,147 @@ int device_op_code(const zlfft_plan_s* p, int op) {
 }
 
 bool aligned(const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(ptr) % a) == 0; }
+
+// Scratch for the multi-pass orders: two buffers of `chunk` transforms. The
+// chunk is sized so that one chunk's intermediates (both buffers) stay in
+// L2 between the passes; it is reused chunk after chunk.
+int ensure_scratch(zlfft_plan_s* p) {
+    if (p->d_scratch) return ZLFFT_OK;
+    const size_t cx = 2 * p->esize;
+    const size_t n = size_t{1} << p->cfft_order;
+    const size_t per = n * cx;
+    size_t chunk = (24u << 20) / per;
+    if (chunk == 0) chunk = 1;
+    const size_t bytes = 2 * chunk * per;
+    if (cudaMalloc(&p->d_scratch, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ZLFFT_ERR_ALLOC, "scratch allocation of %zu bytes failed", bytes);
+    }
+    p->scratch_bytes = bytes;
+    p->chunk = chunk;
+    return ZLFFT_OK;
+}
+
+template <typename F>
+cudaError_t launch_split(const zlfft_plan_s* p, int dop, int out_layout, const void* z, void* o0, void* o1,
+                         long long batch, long long out_stride, cudaStream_t st, const zlfft::LaunchCtx& ctx) {
+    using C = zlfft::Cx<F>;
+    const int M = 1 << p->cfft_order;
+    const long long total = (long long)(M / 2 + 1) * batch;
+    const unsigned grid = (unsigned)std::min<long long>((total + 255) / 256, (long long)p->num_sms * 16);
+    const C* zc = static_cast<const C*>(z);
+    const C* rw = static_cast<const C*>(p->d_rw);
+    if (dop == zlfft::kR2CSqrMag)
+        zlfft::rfft_split_kernel<F, zlfft::kR2CSqrMag, zlfft::kAoS><<<grid, 256, 0, st>>>(zc, o0, o1, rw, M, batch, M, out_stride);
+    else if (out_layout == ZLFFT_AOS)
+        zlfft::rfft_split_kernel<F, zlfft::kR2CFwd, zlfft::kAoS><<<grid, 256, 0, st>>>(zc, o0, o1, rw, M, batch, M, out_stride);
+    else
+        zlfft::rfft_split_kernel<F, zlfft::kR2CFwd, zlfft::kSoA><<<grid, 256, 0, st>>>(zc, o0, o1, rw, M, batch, M, out_stride);
+    if (ctx.launches) ++*ctx.launches;
+    return cudaGetLastError();
+}
+
+template <typename F>
+cudaError_t launch_pre(const zlfft_plan_s* p, int in_layout, const void* i0, const void* i1, void* z, long long batch,
+                       long long in_stride, cudaStream_t st, const zlfft::LaunchCtx& ctx) {
+    using C = zlfft::Cx<F>;
+    const int M = 1 << p->cfft_order;
+    const long long total = (long long)(M / 2 + 1) * batch;
+    const unsigned grid = (unsigned)std::min<long long>((total + 255) / 256, (long long)p->num_sms * 16);
+    const C* rw = static_cast<const C*>(p->d_rw);
+    if (in_layout == ZLFFT_AOS)
+        zlfft::rfft_pre_kernel<F, zlfft::kAoS><<<grid, 256, 0, st>>>(i0, i1, static_cast<C*>(z), rw, M, batch, in_stride, M);
+    else
+        zlfft::rfft_pre_kernel<F, zlfft::kSoA><<<grid, 256, 0, st>>>(i0, i1, static_cast<C*>(z), rw, M, batch, in_stride, M);
+    if (ctx.launches) ++*ctx.launches;
+    return cudaGetLastError();
+}
+
+// Orders above the tile kernel: chunks of transforms through 2-3 Stockham
+// passes (zlfft_pass.cuh); RFFT orders add the split (forward) or the
+// pre-step (backward) as a separate elementwise kernel on the N/2-point
+// spectrum, with the reference's arithmetic.
+int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, const zlfft::TileArgs& a,
+                   cudaStream_t st, const zlfft::LaunchCtx& ctx) {
+    const int P = p->cfft_order;
+    if (P < zlfft::kPassMinP || P > zlfft::kPassMaxP)
+        return fail(ZLFFT_ERR_UNSUPPORTED, "order %d is above the supported maximum", p->order);
+    int rc = ensure_scratch(p);
+    if (rc) return rc;
+    const zlfft::PassTable& t = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
+    const auto& row = t.fn[P - zlfft::kPassMinP];
+    int np = 0;
+    while (np < zlfft::kMaxPasses && row[np][1][0][0]) ++np;
+    const size_t cx = 2 * p->esize;
+    const long long n = 1LL << P;
+    char* s0 = static_cast<char*>(p->d_scratch);
+    char* s1 = s0 + p->scratch_bytes / 2;
+    const bool fwd = (dop == zlfft::kC2CFwd || dop == zlfft::kR2CFwd || dop == zlfft::kR2CSqrMag);
+    const bool r2c = (dop == zlfft::kR2CFwd || dop == zlfft::kR2CSqrMag);
+    const bool c2r = (dop == zlfft::kC2RBwd);
+    const int il = (r2c) ? ZLFFT_AOS : in_layout;   // R2C: real input read as complex pairs
+    const int ol = (c2r) ? ZLFFT_AOS : out_layout;  // C2R: real output written as complex pairs
+    const size_t in_elem = (in_layout == ZLFFT_SOA && !r2c) ? p->esize : cx;
+    const size_t out_elem = (out_layout == ZLFFT_SOA && !c2r) ? p->esize : cx;
+    for (long long b0 = 0; b0 < a.batch; b0 += (long long)p->chunk) {
+        const long long nb = std::min<long long>((long long)p->chunk, a.batch - b0);
+        // this chunk's user buffers
+        const char* ui0 = static_cast<const char*>(a.in0) + b0 * a.in_stride * in_elem;
+        const char* ui1 = a.in1 ? static_cast<const char*>(a.in1) + b0 * a.in_stride * in_elem : nullptr;
+        char* uo0 = static_cast<char*>(a.out0) + b0 * a.out_stride * (dop == zlfft::kR2CSqrMag ? p->esize : out_elem);
+        char* uo1 = a.out1 ? static_cast<char*>(a.out1) + b0 * a.out_stride * out_elem : nullptr;
+        cudaError_t e;
+        // CFFT source/destination for this chunk
+        const void* src0 = ui0;
+        const void* src1 = ui1;
+        long long src_stride = a.in_stride;
+        int src_layout = il;
+        if (c2r) {
+            e = p->prec == ZLFFT_F32 ? launch_pre<float>(p, in_layout, ui0, ui1, s0, nb, a.in_stride, st, ctx)
+                                     : launch_pre<double>(p, in_layout, ui0, ui1, s0, nb, a.in_stride, st, ctx);
+            if (e != cudaSuccess) return cuda_fail(e, "rfft pre-step launch");
+            src0 = s0;
+            src1 = nullptr;
+            src_stride = n;
+            src_layout = ZLFFT_AOS;
+        }
+        char* bufs[2] = {c2r ? s1 : s0, c2r ? s0 : s1};
+        for (int pi = 0; pi < np; ++pi) {
+            const bool last = (pi + 1 == np);
+            zlfft::PassArgs pa;
+            pa.in0 = src0;
+            pa.in1 = src1;
+            pa.in_stride = src_stride;
+            pa.batch = nb;
+            pa.tws = p->d_tws;
+            if (last && !r2c) {
+                pa.out0 = uo0;
+                pa.out1 = uo1;
+                pa.out_stride = a.out_stride;
+            } else {
+                pa.out0 = bufs[pi & 1];
+                pa.out1 = nullptr;
+                pa.out_stride = n;
+            }
+            const int li = pi == 0 ? src_layout : ZLFFT_AOS;
+            const int lo = (last && !r2c) ? ol : ZLFFT_AOS;
+            zlfft::PassLaunchFn fn = row[pi][fwd ? 1 : 0][li][lo];
+            if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no pass kernel for order %d", p->order);
+            e = fn(pa, st, ctx);
+            if (e != cudaSuccess) return cuda_fail(e, "pass launch");
+            src0 = pa.out0;
+            src1 = nullptr;
+            src_stride = n;
+        }
+        if (r2c) {
+            e = p->prec == ZLFFT_F32
+                    ? launch_split<float>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx)
+                    : launch_split<double>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx);
+            if (e != cudaSuccess) return cuda_fail(e, "rfft split launch");
+        }
+    }
+    return ZLFFT_OK;
+}
 
 int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,
                      void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, cudaStream_t stream) {
@@ -271,8 +424,11 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     const int dop = device_op_code(p, op);
     const int P = p->cfft_order;
     zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
+    if (P > zlfft::kTileMaxP) {
+        DeviceGuard g(p->device);
+        return exec_multipass(p, dop, in_layout, out_layout, a, stream, ctx);
+    }
     const zlfft::TileTable& t = p->prec == ZLFFT_F32 ? tables().f32 : tables().f64;
-    if (P > zlfft::kTileMaxP) return fail(ZLFFT_ERR_UNSUPPORTED, "order %d not supported yet", p->order);
     zlfft::TileLaunchFn fn = t.fn[P][dop][in_layout][out_layout];
     if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no kernel for this configuration");
     DeviceGuard g(p->device);
@@ -405,7 +561,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
         return fail(ZLFFT_ERR_INVALID_ARG, "RFFT order must be >= 1 (the reference underflows at 0)");
     if (mode != ZLFFT_MODE_PLAIN) return fail(ZLFFT_ERR_UNSUPPORTED, "mode %d not available", mode);
     const int cfft_order = kind == ZLFFT_C2C ? (int)order : (int)order - 1;
-    if (cfft_order > zlfft::kTileMaxP) return fail(ZLFFT_ERR_UNSUPPORTED, "order %zu not supported yet", order);
+    if (cfft_order > zlfft::kPassMaxP) return fail(ZLFFT_ERR_UNSUPPORTED, "order %zu above the supported maximum", order);
 
     auto* p = new zlfft_plan_s();
     p->kind = kind;

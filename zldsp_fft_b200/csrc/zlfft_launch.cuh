@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include "zlfft_pass.cuh"
 #include "zlfft_tile.cuh"
 
 namespace zlfft {
@@ -46,6 +47,101 @@ cudaError_t launch_tile(const TileArgs& a, cudaStream_t stream, const LaunchCtx&
     kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(a);
     if (ctx.launches) ++*ctx.launches;
     return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ multi-pass
+constexpr int kPassMinP = 14;
+constexpr int kPassMaxP = 24;
+constexpr int kMaxPasses = 3;
+
+using PassLaunchFn = cudaError_t (*)(const PassArgs&, cudaStream_t, const LaunchCtx&);
+
+struct PassTable {
+    // [order - kPassMinP][pass][fwd][in_layout][out_layout]; the layouts only
+    // matter on the first (input) and last (output) pass.
+    PassLaunchFn fn[kPassMaxP - kPassMinP + 1][kMaxPasses][2][2][2];
+};
+
+template <typename F, int P, int PI, bool FWD, int IL, int OL>
+cudaError_t launch_pass(const PassArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
+    using Cfg = PassCfg<F, P, PI>;
+    auto kern = pass_kernel<F, P, PI, FWD, IL, OL>;
+    static const int blocks_per_sm = [kern]() {
+        if (Cfg::SMEM > 48 * 1024)
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, Cfg::THREADS, Cfg::SMEM) != cudaSuccess || b < 1)
+            b = 1;
+        return b;
+    }();
+    if (a.batch <= 0) return cudaSuccess;
+    const long long items = a.batch * Cfg::CPT;
+    const long long cap = (long long)ctx.num_sms * blocks_per_sm;
+    const unsigned grid = (unsigned)(items < cap ? items : cap);
+    kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(a);
+    if (ctx.launches) ++*ctx.launches;
+    return cudaGetLastError();
+}
+
+template <typename F, int P, int PI>
+void fill_pass_one(PassTable& t) {
+    constexpr int np = pass_count(P);
+    constexpr bool first = PI == 0, last = PI + 1 == np;
+    for (int f = 0; f < 2; ++f)
+        for (int il = 0; il < 2; ++il)
+            for (int ol = 0; ol < 2; ++ol) t.fn[P - kPassMinP][PI][f][il][ol] = nullptr;
+    // direction only matters on the first (load swap) and last (store swap) pass
+    auto& e = t.fn[P - kPassMinP][PI];
+    if constexpr (first) {
+        e[1][kAoS][kAoS] = launch_pass<F, P, PI, true, kAoS, kAoS>;
+        e[1][kSoA][kAoS] = launch_pass<F, P, PI, true, kSoA, kAoS>;
+        e[0][kAoS][kAoS] = launch_pass<F, P, PI, false, kAoS, kAoS>;
+        e[0][kSoA][kAoS] = launch_pass<F, P, PI, false, kSoA, kAoS>;
+        e[1][kAoS][kSoA] = e[1][kAoS][kAoS];
+        e[1][kSoA][kSoA] = e[1][kSoA][kAoS];
+        e[0][kAoS][kSoA] = e[0][kAoS][kAoS];
+        e[0][kSoA][kSoA] = e[0][kSoA][kAoS];
+    } else if constexpr (last) {
+        e[1][kAoS][kAoS] = launch_pass<F, P, PI, true, kAoS, kAoS>;
+        e[1][kAoS][kSoA] = launch_pass<F, P, PI, true, kAoS, kSoA>;
+        e[0][kAoS][kAoS] = launch_pass<F, P, PI, false, kAoS, kAoS>;
+        e[0][kAoS][kSoA] = launch_pass<F, P, PI, false, kAoS, kSoA>;
+        e[1][kSoA][kAoS] = e[1][kAoS][kAoS];
+        e[1][kSoA][kSoA] = e[1][kAoS][kSoA];
+        e[0][kSoA][kAoS] = e[0][kAoS][kAoS];
+        e[0][kSoA][kSoA] = e[0][kAoS][kSoA];
+    } else {
+        for (int f = 0; f < 2; ++f)
+            for (int il = 0; il < 2; ++il)
+                for (int ol = 0; ol < 2; ++ol) e[f][il][ol] = launch_pass<F, P, PI, true, kAoS, kAoS>;
+    }
+}
+
+template <typename F, int P>
+void fill_pass_order(PassTable& t) {
+    fill_pass_one<F, P, 0>(t);
+    fill_pass_one<F, P, 1>(t);
+    if constexpr (pass_count(P) > 2) fill_pass_one<F, P, 2>(t);
+}
+
+template <typename F, int... Ps>
+void fill_pass_orders(PassTable& t, std::integer_sequence<int, Ps...>) {
+    (fill_pass_order<F, kPassMinP + Ps>(t), ...);
+}
+
+// ranges split over translation units for parallel builds
+void fill_pass_f32_a(PassTable& t);  // orders 14..18
+void fill_pass_f32_b(PassTable& t);  // orders 19..24
+void fill_pass_f64_a(PassTable& t);
+void fill_pass_f64_b(PassTable& t);
+
+template <typename F, int Lo, int Hi, int... Ps>
+void fill_pass_range_impl(PassTable& t, std::integer_sequence<int, Ps...>) {
+    (fill_pass_order<F, Lo + Ps>(t), ...);
+}
+template <typename F, int Lo, int Hi>
+void fill_pass_range(PassTable& t) {
+    fill_pass_range_impl<F, Lo, Hi>(t, std::make_integer_sequence<int, Hi - Lo + 1>{});
 }
 
 // Each translation unit fills its part of a precision's table.

@@ -1,0 +1,284 @@
+// G4: multi-pass Stockham FFT for transforms too large for one CTA.
+//
+// The reference's stage sequence for order P (radix-8 or radix-4 first pass,
+// then radix-4 passes; src/common/zldsp_fft_common_init.hpp:193-206) is cut
+// into 2 or 3 kernel passes over the same stage groups the tile kernel uses.
+// A pass covering the stages from sub-length L_in to L_out = L_in * R works
+// on "units" U = J * L_in + k (J < N / L_out, k < L_in): the R elements
+// Y_{L_in}[J + rho * N / L_out][k] form a closed Stockham FFT of length R over
+// rho whose twiddles are the global ones, W_{4L}^{q (k + L_in * k_local)}.
+// Unit U reads positions U + pos * N / R and writes positions
+// J * L_out + k + pos * L_in (pos < R), so the passes compose exactly to the
+// reference's arithmetic: results are bit-identical to the single-CTA kernel.
+//
+// Layout in shared memory: element (pos, unit slot u) at pos * ROW + u with
+// ROW = UPC + 1. Lanes run over units fastest, so every read, exchange write
+// and global access of a half-warp touches 16 consecutive units (128 bytes
+// of f32 complex) of one position, and the padded row also makes the
+// column-wise copy-out of the first pass conflict-free.
+//
+// The first pass (sub-length 1 -> R) writes each unit's R results
+// contiguously, so its CTA output is one contiguous block, copied out of
+// shared memory with coalesced stores. Later passes store straight from
+// registers (consecutive units are consecutive positions).
+#pragma once
+
+#include "zlfft_tile.cuh"
+
+namespace zlfft {
+
+// Passes for order P: from the end, pairs of radix-16 groups (256 points)
+// form passes until the remaining leading groups fit 1024 points.
+__host__ __device__ constexpr int pass_count(int P) {
+    const int ng = tile_num_groups(P);
+    int end = ng, n = 0;
+    while (true) {
+        int prod = 1;
+        for (int g = 0; g < end; ++g) prod *= tile_group(P, g).R;
+        if (prod <= 1024 || end <= 2) return n + 1;
+        end -= 2;
+        ++n;
+    }
+}
+
+// First group index of pass i (0-based); pass i covers groups [pass_gb(i), pass_gb(i + 1)).
+__host__ __device__ constexpr int pass_gb(int P, int i) {
+    const int ng = tile_num_groups(P);
+    const int np = pass_count(P);
+    if (i >= np) return ng;
+    if (i == 0) return 0;
+    // passes 1..np-1 are pairs of radix-16 groups at the end
+    return ng - 2 * (np - i);
+}
+
+__host__ __device__ constexpr int pass_radix(int P, int i) {
+    int r = 1;
+    for (int g = pass_gb(P, i); g < pass_gb(P, i + 1); ++g) r *= tile_group(P, g).R;
+    return r;
+}
+
+template <typename F, int P, int PI>
+struct PassCfg {
+    using C = Cx<F>;
+    static constexpr int N = 1 << P;
+    static constexpr int GB = pass_gb(P, PI);
+    static constexpr int GE = pass_gb(P, PI + 1);
+    static constexpr int R = pass_radix(P, PI);
+    static constexpr int L_IN = tile_group(P, GB).L;
+    static constexpr int L_OUT = L_IN * R;
+    static constexpr bool FIRST = (PI == 0);
+    static constexpr bool LAST = (GE == tile_num_groups(P));
+    static constexpr int E = [] {
+        int e = 1;
+        for (int g = GB; g < GE; ++g) e = tile_group(P, g).R > e ? tile_group(P, g).R : e;
+        return e;
+    }();
+    static constexpr int T = R / E;  // threads per unit
+    static constexpr int UMIN = 128 / (int)sizeof(C);  // units per 128-byte row
+    static constexpr int UPC = (128 * E / R) > UMIN ? (128 * E / R) : UMIN;  // units per CTA
+    static constexpr int ROW = UPC + 1;
+    static constexpr int THREADS = UPC * T;
+    static constexpr size_t SMEM = (size_t)R * ROW * sizeof(C);
+    static constexpr int UNITS = N / R;            // units per transform
+    static constexpr int CPT = UNITS / UPC;        // CTAs (work items) per transform
+    static constexpr int MINB = (65536 / (THREADS * 96)) > 0 ? (65536 / (THREADS * 96)) : 1;
+    static_assert(UNITS % UPC == 0, "a transform must split into whole CTAs");
+    static_assert(SMEM <= 200 * 1024, "pass tile too large");
+};
+
+struct PassArgs {
+    const void* in0;  // first pass: user input (layout IL); else scratch (AoS complex)
+    const void* in1;
+    void* out0;       // last pass: user output (layout OL); else scratch (AoS complex)
+    void* out1;
+    long long batch;
+    long long in_stride;   // elements between transforms of the input
+    long long out_stride;  // elements between transforms of the output
+    const void* tws;       // per-stage twiddle tables (stage_l0 layout)
+};
+
+// One pass over `batch` transforms. FWD selects the direction swap on the
+// first pass's loads and the last pass's stores (the reference's backward
+// transform is swap(DFT(swap(x))), src/common/zldsp_fft_common_structure.hpp:47-95).
+template <typename F, int P, int PI, bool FWD, int IL, int OL>
+__global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>::MINB) pass_kernel(const PassArgs a) {
+    using Cfg = PassCfg<F, P, PI>;
+    using C = Cx<F>;
+    constexpr int N = Cfg::N, R = Cfg::R, E = Cfg::E, T = Cfg::T, UPC = Cfg::UPC, ROW = Cfg::ROW;
+    constexpr int L_IN = Cfg::L_IN, L_OUT = Cfg::L_OUT, GB = Cfg::GB, GE = Cfg::GE;
+    constexpr int IL2 = Cfg::FIRST ? IL : (int)kAoS;
+    constexpr int OL2 = Cfg::LAST ? OL : (int)kAoS;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw);
+    const int u = (int)threadIdx.x % UPC;
+    const int tb = (int)threadIdx.x / UPC;
+    const C* tws = static_cast<const C*>(a.tws);
+    const long long items = a.batch * Cfg::CPT;
+
+    for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+        const long long tr = item / Cfg::CPT;
+        const int U = (int)(item % Cfg::CPT) * UPC + u;
+        const int ku = U % L_IN;  // k of the unit
+        const int J = U / L_IN;
+        C v[E];
+
+        [&]<int... GI>(std::integer_sequence<int, GI...>) {
+            (
+                [&] {
+                    constexpr int g = GB + GI;
+                    constexpr Grp G = tile_group(P, g);
+                    constexpr int NB = E / G.R;
+                    constexpr int ELL = G.L / L_IN;  // local sub-length at group entry
+                    constexpr bool kLastG = (g + 1 == GE);
+                    // ---- inputs
+                    if constexpr (GI == 0) {
+                        const CxIn<F, IL2> in(a.in0, a.in1, tr * a.in_stride);
+#pragma unroll
+                        for (int i = 0; i < NB; ++i) {
+                            const int b = tb + i * T;
+#pragma unroll
+                            for (int rho = 0; rho < G.R; ++rho) {
+                                const int pos = b + rho * (R / G.R);
+                                C x = in[U + pos * (N / R)];
+                                v[i * G.R + rho] = (Cfg::FIRST && !FWD) ? cswap(x) : x;
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < NB; ++i) {
+                            const int b = tb + i * T;
+#pragma unroll
+                            for (int rho = 0; rho < G.R; ++rho) v[i * G.R + rho] = sm[(b + rho * (R / G.R)) * ROW + u];
+                        }
+                    }
+                    // ---- compute (global twiddles: kk = ku + L_IN * k_local)
+#pragma unroll
+                    for (int i = 0; i < NB; ++i) {
+                        const int b = tb + i * T;
+                        const uint32_t kk = (uint32_t)(ku + L_IN * (b % ELL));
+                        group_compute_ld<P, G.R, G.L, G.first>(v + i * G.R, kk, tws);
+                    }
+                    // ---- outputs
+                    if constexpr (!kLastG) {
+                        __syncthreads();
+#pragma unroll
+                        for (int i = 0; i < NB; ++i) {
+                            const int b = tb + i * T;
+                            const int Jl = b / ELL, kl = b % ELL;
+#pragma unroll
+                            for (int s = 0; s < G.R; ++s)
+                                sm[(Jl * G.R * ELL + kl + group_mu(G, s) * ELL) * ROW + u] = v[i * G.R + s];
+                        }
+                        __syncthreads();
+                    } else if constexpr (L_IN == 1) {
+                        // first pass: each unit's outputs are contiguous; stage them and copy
+                        // the CTA's block (UPC units x R) out with consecutive threads on
+                        // consecutive elements.
+                        __syncthreads();
+#pragma unroll
+                        for (int i = 0; i < NB; ++i) {
+                            const int b = tb + i * T;  // J_local == 0 in the last group
+#pragma unroll
+                            for (int s = 0; s < G.R; ++s) sm[(b + group_mu(G, s) * ELL) * ROW + u] = v[i * G.R + s];
+                        }
+                        __syncthreads();
+                        const CxOut<F, OL2> out(a.out0, a.out1, tr * a.out_stride + (long long)(U - u) * R);
+#pragma unroll 4
+                        for (int e = (int)threadIdx.x; e < UPC * R; e += Cfg::THREADS) {
+                            const int uu = e / R, pos = e % R;
+                            const C x = sm[pos * ROW + uu];
+                            out.put(e, (Cfg::LAST && !FWD) ? cswap(x) : x);
+                        }
+                        __syncthreads();
+                    } else {
+                        const CxOut<F, OL2> out(a.out0, a.out1, tr * a.out_stride + (long long)J * L_OUT + ku);
+#pragma unroll
+                        for (int i = 0; i < NB; ++i) {
+                            const int b = tb + i * T;
+#pragma unroll
+                            for (int s = 0; s < G.R; ++s) {
+                                const int pos = b + group_mu(G, s) * ELL;
+                                const C x = v[i * G.R + s];
+                                out.put(pos * L_IN, (Cfg::LAST && !FWD) ? cswap(x) : x);
+                            }
+                        }
+                    }
+                }(),
+                ...);
+        }(std::make_integer_sequence<int, GE - GB>{});
+        // shared memory is rewritten by the next item's first exchange only after a barrier
+    }
+}
+
+// ---------------------------------------------------------------- RFFT split / pre-step
+// Stand-alone forms for the multi-pass orders: the forward split reads the
+// N/2-point spectrum Z (AoS, natural order) and writes bins (or squared
+// magnitudes); the backward pre-step writes Z from bins
+// (src/common/zldsp_fft_common_execute.hpp:318-368, :481-536, :399-451).
+// One thread per bin pair (k, M - k), k = 0 .. M/2 (k = 0 is DC/Nyquist).
+template <typename F, int OP, int LAYOUT>
+__global__ void rfft_split_kernel(const Cx<F>* z, void* out0, void* out1, const Cx<F>* rw, int M, long long batch,
+                                  long long z_stride, long long out_stride) {
+    using C = Cx<F>;
+    const long long pairs = (long long)(M / 2 + 1);
+    const long long total = pairs * batch;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long tr = i / pairs;
+        const int k = (int)(i % pairs);
+        const C* zt = z + tr * z_stride;
+        constexpr int OL2 = (OP == kR2CSqrMag) ? (int)kAoS : LAYOUT;
+        const CxOut<F, OL2> out(out0, out1, tr * out_stride);
+        F* osq = static_cast<F*>(out0) + tr * out_stride;
+        if (k == 0) {
+            const C z0 = zt[0];
+            const F dc = z0.x + z0.y, ny = z0.x - z0.y;
+            if constexpr (OP == kR2CFwd) {
+                out.put(0, cx<C>(dc, (F)0));
+                out.put(M, cx<C>(ny, (F)0));
+            } else {
+                osq[0] = mul_rn(dc, dc);
+                osq[M] = mul_rn(ny, ny);
+            }
+            continue;
+        }
+        const C w = rw[k];
+        const SplitOut<F> o = rfft_split<F>(zt[k], zt[M - k], w.x, w.y);
+        if constexpr (OP == kR2CFwd) {
+            if (k != M / 2) out.put(k, cx<C>(o.xr_k, o.xi_k));
+            out.put(M - k, cx<C>(o.xr_m, o.xi_m));
+        } else {
+            if (k != M / 2) osq[k] = fma_rn(o.xr_k, o.xr_k, mul_rn(o.xi_k, o.xi_k));
+            osq[M - k] = fma_rn(o.xr_m, o.xr_m, mul_rn(o.xi_m, o.xi_m));
+        }
+    }
+}
+
+template <typename F, int LAYOUT>
+__global__ void rfft_pre_kernel(const void* in0, const void* in1, Cx<F>* z, const Cx<F>* rw, int M, long long batch,
+                                long long in_stride, long long z_stride) {
+    using C = Cx<F>;
+    const long long pairs = (long long)(M / 2 + 1);
+    const long long total = pairs * batch;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long tr = i / pairs;
+        const int k = (int)(i % pairs);
+        const CxIn<F, LAYOUT> in(in0, in1, tr * in_stride);
+        C* zt = z + tr * z_stride;
+        if (k == 0) {
+            const C x0 = in[0], xm = in[M];
+            zt[0] = cx<C>(mul_rn(x0.x + xm.x, (F)0.5), mul_rn(x0.x - xm.x, (F)0.5));
+            continue;
+        }
+        const C x1 = in[k], x2 = in[M - k];
+        const C w = rw[k];
+        const F c = w.x, s = w.y;
+        const F si = x1.y + x2.y, dr = x1.x - x2.x;
+        const C zk = cx<C>(fma_rn(-dr, s, fma_rn(-si, c, x1.x)), fma_rn(dr, c, fma_rn(-si, s, x1.y)));
+        const C zm = cx<C>(fma_rn(dr, s, fma_rn(si, c, x2.x)), fma_rn(dr, c, fma_rn(-si, s, x2.y)));
+        if (k != M / 2) zt[k] = zk;
+        zt[M - k] = zm;
+    }
+}
+
+}  // namespace zlfft
