@@ -213,6 +213,9 @@ class Rfft12:
     def take_launches(self):
         return self.plan.take_launch_count()
 
+    def cpu_sample_desc(self, frames):
+        return f"{frames} of {self.batch} frames, same ops as one step, median of 3"
+
     # ---- end to end through the host API (pinned host buffers)
     def setup_e2e(self):
         import torch
@@ -256,7 +259,108 @@ class Rfft12:
         return self.bytes_per_step * frames / self.batch, dt
 
 
-WORKLOADS = {"rfft12": Rfft12}
+class Cfft2G:
+    """CFFT<float> orders 14, 16 and 20, each batched to 2 GiB of complex64
+    input (batch 16384 / 4096 / 256); one step = forward then backward of all
+    three (plain FP32 form). re, im ~ U[-1, 1), seed 1003."""
+    name = "cfft2g"
+    desc = "CFFT<float> orders 14/16/20 x 2 GiB complex64 each (batch 16384/4096/256), forward + backward"
+    orders = (14, 16, 20)
+    total = 1 << 28  # complex elements per order (2 GiB)
+    dtype = "f32"
+
+    def __init__(self, total_log2=28):
+        self.total = 1 << total_log2
+        self.op_bytes = {}
+        for o in self.orders:
+            for d in ("fwd", "bwd"):
+                self.op_bytes[f"c2c_{d}_order{o}"] = 2 * 8 * self.total  # read + write
+        self.bytes_per_step = sum(self.op_bytes.values())
+        self.dominant = "c2c_fwd_order16"
+
+    def setup(self, device):
+        import torch
+        import zldsp_fft_b200 as Z
+        self.Z = Z
+        self.plans = {o: Z.Plan(Z.C2C, o, np.float32, device=device) for o in self.orders}
+        g = torch.Generator(device=device)
+        g.manual_seed(1003)
+        # A: input (never overwritten), B: forward output, C: backward output
+        self.A = (torch.rand((self.total, 2), generator=g, device=device) * 2 - 1).contiguous()
+        self.B = torch.empty_like(self.A)
+        self.C = torch.empty_like(self.A)
+        torch.cuda.synchronize(device)
+        self.host_in = None
+
+    def ops(self, step):
+        Z = self.Z
+        out = []
+        for o in self.orders:
+            p = self.plans[o]
+            b = self.total >> o
+
+            def fwd(st, p=p, b=b):
+                p.exec_device(Z.FORWARD, Z.AOS, Z.AOS, self.A.data_ptr(), None, self.B.data_ptr(), None, b, stream=st)
+
+            def bwd(st, p=p, b=b):
+                p.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, self.B.data_ptr(), None, self.C.data_ptr(), None, b, stream=st)
+
+            out += [(f"c2c_fwd_order{o}", fwd), (f"c2c_bwd_order{o}", bwd)]
+        return out
+
+    def take_launches(self):
+        return sum(p.take_launch_count() for p in self.plans.values())
+
+    batch = 1 << 14  # largest per-order batch (order 14), for sample sizing
+
+    def cpu_sample_desc(self, frames):
+        cnt = [max(1, min(frames >> max(0, o - 14), self.total >> o)) for o in self.orders]
+        return (f"forward+backward of {cnt[0]}/{cnt[1]}/{cnt[2]} transforms of orders 14/16/20 "
+                f"(of 16384/4096/256 per step), median of 3")
+
+    def setup_e2e(self):
+        import torch
+        # host copies of A, pinned; forward into hB, backward in place in hB
+        self.hA = self.A.cpu().pin_memory()
+        self.hB = torch.empty_like(self.hA).pin_memory()
+        self.e2e_h2d = 2 * 8 * self.total * len(self.orders)
+        self.e2e_d2h = 2 * 8 * self.total * len(self.orders)
+
+    def e2e_step(self):
+        Z = self.Z
+        for o in self.orders:
+            p = self.plans[o]
+            b = self.total >> o
+            p.exec_host(Z.FORWARD, Z.AOS, Z.AOS, self.hA.data_ptr(), None, self.hB.data_ptr(), None, b)
+            p.exec_host(Z.BACKWARD, Z.AOS, Z.AOS, self.hB.data_ptr(), None, self.hB.data_ptr(), None, b)
+
+    def cpu_run(self, frames, threads, kind):
+        """`frames` transforms of each order (forward + backward) on the CPU."""
+        from oracle import oracle as O
+        rng = np.random.default_rng(1003)
+        nbytes, dt = 0.0, 0.0
+        for o in self.orders:
+            n = 1 << o
+            cnt = max(1, min(frames >> max(0, o - 14), self.total >> o))
+            x = (rng.uniform(-1, 1, (cnt, n)) + 1j * rng.uniform(-1, 1, (cnt, n))).astype(np.complex64)
+            if kind == "reference":
+                plan = O.RefPlan("c2c", o, "f32", threads)
+                y = np.empty_like(x)
+                z = np.empty_like(x)
+                t0 = time.perf_counter()
+                plan.cfft(x, True, out=y)
+                plan.cfft(y, False, out=z)
+                dt += time.perf_counter() - t0
+                plan.close()
+            else:
+                t0 = time.perf_counter()
+                O.cfft_port(O.cfft_port(x, True), False)
+                dt += time.perf_counter() - t0
+            nbytes += 2 * 2 * 8 * n * cnt
+        return nbytes, dt
+
+
+WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G}
 
 
 # ------------------------------------------------------------------ CPU baseline
@@ -265,8 +369,8 @@ def cpu_baseline(wl, target_s=3.0, threads=None, kind=None):
     if kind is None:
         kind = "reference" if O.ref_available() else "port"
     threads = threads or (os.cpu_count() or 1) if kind == "reference" else 1
-    frames = 64
-    avail = wl.host_in.shape[0]
+    frames = 64 if wl.host_in is None else 64
+    avail = wl.batch if wl.host_in is None else wl.host_in.shape[0]
     nbytes, dt = wl.cpu_run(frames, threads, kind)
     while dt < target_s / 4 and frames < avail:
         frames = min(avail, frames * 4)
@@ -277,7 +381,7 @@ def cpu_baseline(wl, target_s=3.0, threads=None, kind=None):
     gbs = statistics.median(b / t / 1e9 for b, t in runs)
     return {
         "value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-        "sample": f"{frames} of {wl.batch} frames, same ops as one step, median of 3",
+        "sample": wl.cpu_sample_desc(frames),
     }
 
 
@@ -291,11 +395,12 @@ def run_reference_arm(args, wl_cls):
     kind = "reference" if O.ref_available() else "port"
     threads = os.cpu_count() or 1
     wl.host_in = hann_frames(min(wl.batch, 2048), wl.n, 1002) if hasattr(wl, "n") else None
+    avail = wl.host_in.shape[0] if wl.host_in is not None else wl.batch
     # each step: a bounded sample of the workload on all host cores
-    frames = 64
+    frames = 16
     _, dt = wl.cpu_run(frames, threads, kind)
-    while dt < 0.25 and frames < wl.host_in.shape[0]:
-        frames = min(wl.host_in.shape[0], frames * 2)
+    while dt < 0.25 and frames < avail:
+        frames = min(avail, frames * 2)
         _, dt = wl.cpu_run(frames, threads, kind)
     for _ in range(args.warmup):
         wl.cpu_run(frames, threads, kind)
@@ -309,9 +414,9 @@ def run_reference_arm(args, wl_cls):
         "metric": METRIC, "value": round(v, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * tot_t / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic",
-        "config": {"workload": wl.desc, "sample_frames_per_step": frames},
+        "config": {"workload": wl.desc},
         "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-                         "sample": f"{frames} of {wl.batch} frames per step, same ops"},
+                         "sample": wl.cpu_sample_desc(frames) + " per step"},
         "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -433,10 +538,17 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rfft12")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cfft2g")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--total-log2", type=int, default=None,
+                    help="cfft2g only: complex elements per order = 2^k (default 28 = 2 GiB); smaller cases "
+                         "are for profiling and are not the benchmark configuration")
     args = ap.parse_args()
     wl_cls = WORKLOADS[args.workload]
+    if args.total_log2 is not None:
+        base = wl_cls
+        wl_cls = lambda: base(total_log2=args.total_log2)  # noqa: E731
+        wl_cls.__name__ = base.__name__
     if args.impl == "reference":
         return run_reference_arm(args, wl_cls)
     return run_ours(args, wl_cls)

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -158,6 +159,8 @@ struct zlfft_plan_s {
     // multi-pass scratch (two buffers of `chunk` transforms each)
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
+    cudaStream_t lanes[2] = {nullptr, nullptr};  // chunk pipelines (alternate chunks)
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     size_t chunk = 0;  // transforms per chunk; intermediates of one chunk stay L2-resident
     int* d_err = nullptr;  // device error word written by kernels (bounded waits that ran out)
     std::mutex mu;
@@ -184,6 +187,11 @@ void release(zlfft_plan p) {
     if (p->d_rw) cudaFree(p->d_rw);
     if (p->d_err) cudaFree(p->d_err);
     if (p->d_scratch) cudaFree(p->d_scratch);
+    for (int i = 0; i < 2; ++i) {
+        if (p->lanes[i]) cudaStreamDestroy(p->lanes[i]);
+        if (p->ev_join[i]) cudaEventDestroy(p->ev_join[i]);
+    }
+    if (p->ev_fork) cudaEventDestroy(p->ev_fork);
     if (p->d_in) cudaFree(p->d_in);
     if (p->d_out) cudaFree(p->d_out);
     if (p->h_in) cudaFreeHost(p->h_in);
@@ -234,15 +242,27 @@ int ensure_scratch(zlfft_plan_s* p) {
     const size_t cx = 2 * p->esize;
     const size_t n = size_t{1} << p->cfft_order;
     const size_t per = n * cx;
-    size_t chunk = (24u << 20) / per;
+    size_t budget = size_t{48} << 20;  // bytes of one scratch buffer (measured plateau: 32-128 MiB)
+    if (const char* env = getenv("ZLFFT_CHUNK_MB")) {
+        const long v = atol(env);
+        if (v > 0) budget = (size_t)v << 20;
+    }
+    size_t chunk = budget / per;
     if (chunk == 0) chunk = 1;
-    const size_t bytes = 2 * chunk * per;
+    const size_t bytes = 4 * chunk * per;  // two buffers for each of the two chunk pipelines
     if (cudaMalloc(&p->d_scratch, bytes) != cudaSuccess) {
         cudaGetLastError();
         return fail(ZLFFT_ERR_ALLOC, "scratch allocation of %zu bytes failed", bytes);
     }
     p->scratch_bytes = bytes;
     p->chunk = chunk;
+    for (int i = 0; i < 2; ++i) {
+        if (cudaStreamCreateWithFlags(&p->lanes[i], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&p->ev_join[i], cudaEventDisableTiming) != cudaSuccess)
+            return fail(ZLFFT_ERR_CUDA, "stream creation failed");
+    }
+    if (cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) != cudaSuccess)
+        return fail(ZLFFT_ERR_CUDA, "event creation failed");
     return ZLFFT_OK;
 }
 
@@ -298,8 +318,8 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
     while (np < zlfft::kMaxPasses && row[np][1][0][0]) ++np;
     const size_t cx = 2 * p->esize;
     const long long n = 1LL << P;
-    char* s0 = static_cast<char*>(p->d_scratch);
-    char* s1 = s0 + p->scratch_bytes / 2;
+    char* s0 = nullptr;
+    char* s1 = nullptr;
     const bool fwd = (dop == zlfft::kC2CFwd || dop == zlfft::kR2CFwd || dop == zlfft::kR2CSqrMag);
     const bool r2c = (dop == zlfft::kR2CFwd || dop == zlfft::kR2CSqrMag);
     const bool c2r = (dop == zlfft::kC2RBwd);
@@ -307,8 +327,24 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
     const int ol = (c2r) ? ZLFFT_AOS : out_layout;  // C2R: real output written as complex pairs
     const size_t in_elem = (in_layout == ZLFFT_SOA && !r2c) ? p->esize : cx;
     const size_t out_elem = (out_layout == ZLFFT_SOA && !c2r) ? p->esize : cx;
-    for (long long b0 = 0; b0 < a.batch; b0 += (long long)p->chunk) {
+    // Chunks alternate between two internal streams forked from (and joined
+    // back to) the caller's stream, so one chunk's passes overlap the other's
+    // launch gaps and wave tails. Each stream owns two scratch buffers.
+    const long long nchunks = (a.batch + (long long)p->chunk - 1) / (long long)p->chunk;
+    const bool fork = nchunks > 1;
+    if (fork) {
+        if (cudaEventRecord(p->ev_fork, st) != cudaSuccess) return fail(ZLFFT_ERR_CUDA, "event record failed");
+        for (int i = 0; i < 2; ++i)
+            if (cudaStreamWaitEvent(p->lanes[i], p->ev_fork, 0) != cudaSuccess)
+                return fail(ZLFFT_ERR_CUDA, "stream wait failed");
+    }
+    const cudaStream_t caller = st;
+    const size_t quarter = p->scratch_bytes / 4;
+    for (long long b0 = 0, ci = 0; b0 < a.batch; b0 += (long long)p->chunk, ++ci) {
         const long long nb = std::min<long long>((long long)p->chunk, a.batch - b0);
+        if (fork) st = p->lanes[ci & 1];
+        s0 = static_cast<char*>(p->d_scratch) + (size_t)(fork ? (ci & 1) : 0) * 2 * quarter;
+        s1 = s0 + quarter;
         // this chunk's user buffers
         const char* ui0 = static_cast<const char*>(a.in0) + b0 * a.in_stride * in_elem;
         const char* ui1 = a.in1 ? static_cast<const char*>(a.in1) + b0 * a.in_stride * in_elem : nullptr;
@@ -338,6 +374,13 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
             pa.in_stride = src_stride;
             pa.batch = nb;
             pa.tws = p->d_tws;
+            pa.err = p->d_err;
+            {
+                // bulk-copy rows need 16-byte aligned sources (bases and transform stride)
+                const size_t eb = (pi == 0 && src_layout == ZLFFT_SOA) ? p->esize : cx;
+                pa.tma = (aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
+                          (nb == 1 || ((size_t)src_stride * eb) % 16 == 0)) ? 1 : 0;
+            }
             if (last && !r2c) {
                 pa.out0 = uo0;
                 pa.out1 = uo1;
@@ -362,6 +405,13 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
                     ? launch_split<float>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx)
                     : launch_split<double>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx);
             if (e != cudaSuccess) return cuda_fail(e, "rfft split launch");
+        }
+    }
+    if (fork) {
+        for (int i = 0; i < 2; ++i) {
+            if (cudaEventRecord(p->ev_join[i], p->lanes[i]) != cudaSuccess ||
+                cudaStreamWaitEvent(caller, p->ev_join[i], 0) != cudaSuccess)
+                return fail(ZLFFT_ERR_CUDA, "stream join failed");
         }
     }
     return ZLFFT_OK;

@@ -3,7 +3,11 @@
 // functions, so the C ABI dispatches with one indexed load.
 #pragma once
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+
+#include <string.h>
 
 #include "zlfft_pass.cuh"
 #include "zlfft_tile.cuh"
@@ -62,10 +66,60 @@ struct PassTable {
     PassLaunchFn fn[kPassMaxP - kPassMinP + 1][kMaxPasses][2][2][2];
 };
 
+// cuTensorMapEncodeTiled, reached through the runtime's driver entry point
+// (no link-time dependency on libcuda).
+inline PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled fn = []() -> PFN_cuTensorMapEncodeTiled {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+    }();
+    return fn;
+}
+
+// Encode the input maps of a pass: {units * comps, R, batch} with strides
+// {N/R * comps, transform stride} scalars; box {UPC * comps, RB, 1}.
+// Returns false (direct loads) when the source does not meet TMA rules.
+template <typename F, int P, int PI, int IL2>
+bool encode_pass_maps(const PassArgs& a, PassMaps& m) {
+    using Cfg = PassCfg<F, P, PI>;
+    if (!Cfg::kTMA) return false;
+    PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+    if (!enc) return false;
+    constexpr int CMP = IL2 == kSoA ? 1 : 2;
+    const CUtensorMapDataType dt = sizeof(F) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const cuuint64_t row_bytes = (cuuint64_t)(Cfg::N / Cfg::R) * CMP * sizeof(F);
+    cuuint64_t tr_bytes = (cuuint64_t)a.in_stride * CMP * sizeof(F);
+    if (a.batch == 1) tr_bytes = (cuuint64_t)Cfg::N * CMP * sizeof(F);
+    if (tr_bytes % 16 != 0 || row_bytes % 16 != 0) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)(Cfg::N / Cfg::R) * CMP, (cuuint64_t)Cfg::R, (cuuint64_t)a.batch};
+    const cuuint64_t strides[2] = {row_bytes, tr_bytes};
+    const cuuint32_t box[3] = {(cuuint32_t)(Cfg::UPC * CMP), (cuuint32_t)Cfg::RB, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const void* bases[2] = {a.in0, IL2 == kSoA ? a.in1 : nullptr};
+    CUtensorMap* maps[2] = {&m.m0, &m.m1};
+    for (int i = 0; i < (IL2 == kSoA ? 2 : 1); ++i) {
+        if (reinterpret_cast<uintptr_t>(bases[i]) % 16 != 0) return false;
+        if (enc(maps[i], dt, 3, const_cast<void*>(bases[i]), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
+
 template <typename F, int P, int PI, bool FWD, int IL, int OL>
-cudaError_t launch_pass(const PassArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
+cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = PassCfg<F, P, PI>;
     auto kern = pass_kernel<F, P, PI, FWD, IL, OL>;
+    constexpr int IL2 = Cfg::FIRST ? IL : (int)kAoS;
+    PassArgs a = a_in;
+    PassMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    a.tma = (a.tma && encode_pass_maps<F, P, PI, IL2>(a, maps)) ? 1 : 0;
     static const int blocks_per_sm = [kern]() {
         if (Cfg::SMEM > 48 * 1024)
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
@@ -78,7 +132,7 @@ cudaError_t launch_pass(const PassArgs& a, cudaStream_t stream, const LaunchCtx&
     const long long items = a.batch * Cfg::CPT;
     const long long cap = (long long)ctx.num_sms * blocks_per_sm;
     const unsigned grid = (unsigned)(items < cap ? items : cap);
-    kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(a);
+    kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(a, maps);
     if (ctx.launches) ++*ctx.launches;
     return cudaGetLastError();
 }

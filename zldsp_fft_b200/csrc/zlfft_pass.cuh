@@ -23,6 +23,8 @@
 // registers (consecutive units are consecutive positions).
 #pragma once
 
+#include <cuda.h>
+
 #include "zlfft_tile.cuh"
 
 namespace zlfft {
@@ -78,7 +80,14 @@ struct PassCfg {
     static constexpr int UPC = (128 * E / R) > UMIN ? (128 * E / R) : UMIN;  // units per CTA
     static constexpr int ROW = UPC + 1;
     static constexpr int THREADS = UPC * T;
-    static constexpr size_t SMEM = (size_t)R * ROW * sizeof(C);
+    static constexpr size_t XBYTES = (size_t)R * ROW * sizeof(C);  // exchange buffer (padded rows)
+    static constexpr size_t SOFF = (XBYTES + 127) / 128 * 128;     // staging offset (128-byte aligned)
+    static constexpr size_t SBYTES = (size_t)R * UPC * sizeof(C);  // staging buffer
+    // The next item's input (a box of UPC units x R positions) is prefetched
+    // by one 3-D tensor copy per 256 positions while the current item computes.
+    static constexpr int RB = R < 256 ? R : 256;  // positions per box
+    static constexpr bool kTMA = SOFF + SBYTES + 16 <= 200 * 1024;
+    static constexpr size_t SMEM = kTMA ? SOFF + SBYTES + 16 : XBYTES;
     static constexpr int UNITS = N / R;            // units per transform
     static constexpr int CPT = UNITS / UPC;        // CTAs (work items) per transform
     static constexpr int MINB = (65536 / (THREADS * 96)) > 0 ? (65536 / (THREADS * 96)) : 1;
@@ -95,13 +104,24 @@ struct PassArgs {
     long long in_stride;   // elements between transforms of the input
     long long out_stride;  // elements between transforms of the output
     const void* tws;       // per-stage twiddle tables (stage_l0 layout)
+    int* err;              // device error word (kDevErrWaitTimeout on a timed-out wait)
+    int tma;               // the tensor maps describe the input (else direct loads)
+};
+
+// Tensor maps of a pass input, encoded on the host (zlfft_launch.cuh): a 3-D
+// view {units * comps, R positions, batch} of the AoS array (comps = 2
+// interleaved re/im scalars) or of each SoA array (comps = 1).
+struct PassMaps {
+    CUtensorMap m0;
+    CUtensorMap m1;
 };
 
 // One pass over `batch` transforms. FWD selects the direction swap on the
 // first pass's loads and the last pass's stores (the reference's backward
 // transform is swap(DFT(swap(x))), src/common/zldsp_fft_common_structure.hpp:47-95).
 template <typename F, int P, int PI, bool FWD, int IL, int OL>
-__global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>::MINB) pass_kernel(const PassArgs a) {
+__global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>::MINB)
+    pass_kernel(const PassArgs a, const __grid_constant__ PassMaps maps) {
     using Cfg = PassCfg<F, P, PI>;
     using C = Cx<F>;
     constexpr int N = Cfg::N, R = Cfg::R, E = Cfg::E, T = Cfg::T, UPC = Cfg::UPC, ROW = Cfg::ROW;
@@ -116,12 +136,57 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
     const C* tws = static_cast<const C*>(a.tws);
     const long long items = a.batch * Cfg::CPT;
 
+    // ---- TMA staging: [pos][u] unpadded (SoA: a re plane then an im plane)
+    constexpr bool kSoAIn = (IL2 == kSoA);
+    constexpr int CMP = kSoAIn ? 1 : 2;  // scalars per unit in the map's innermost dimension
+    C* stage = reinterpret_cast<C*>(smem_raw + Cfg::SOFF);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::SOFF + Cfg::SBYTES);
+    const bool use_tma = Cfg::kTMA && a.tma;
+    auto issue = [&](long long it) {  // one thread issues the item's box copies
+        if (!use_tma || threadIdx.x != 0 || it >= items) return;
+        const int z = (int)(it / Cfg::CPT);
+        const int x = (int)(it % Cfg::CPT) * UPC * CMP;  // x * sizeof(F) = 16-byte multiple
+        mbar_arrive_expect_tx(bar, (uint32_t)Cfg::SBYTES);
+        F* sf = reinterpret_cast<F*>(stage);
+#pragma unroll
+        for (int y = 0; y < R; y += Cfg::RB) {
+            if constexpr (kSoAIn) {
+                tma_load_3d(sf + (size_t)y * UPC, &maps.m0, x, y, z, bar);
+                tma_load_3d(sf + (size_t)R * UPC + (size_t)y * UPC, &maps.m1, x, y, z, bar);
+            } else {
+                tma_load_3d(stage + (size_t)y * UPC, &maps.m0, x, y, z, bar);
+            }
+        }
+    };
+    if constexpr (Cfg::kTMA) {
+        if (use_tma) {
+            if (threadIdx.x == 0) {
+                mbar_init(bar, 1);
+                fence_mbar_init();
+            }
+            __syncthreads();
+            issue(blockIdx.x);
+        }
+    }
+    uint32_t phase = 0;
+
     for (long long item = blockIdx.x; item < items; item += gridDim.x) {
         const long long tr = item / Cfg::CPT;
         const int U = (int)(item % Cfg::CPT) * UPC + u;
         const int ku = U % L_IN;  // k of the unit
         const int J = U / L_IN;
         C v[E];
+        if constexpr (Cfg::kTMA) {
+            if (use_tma) {
+                const bool ok = mbar_wait(bar, phase);
+                if (__syncthreads_or(!ok)) {  // bounded wait ran out: report and leave
+                    if (threadIdx.x == 0) atomicOr(a.err, kDevErrWaitTimeout);
+                    mbar_wait(bar, phase);
+                    return;
+                }
+                phase ^= 1u;
+            }
+        }
 
         [&]<int... GI>(std::integer_sequence<int, GI...>) {
             (
@@ -133,15 +198,32 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                     constexpr bool kLastG = (g + 1 == GE);
                     // ---- inputs
                     if constexpr (GI == 0) {
-                        const CxIn<F, IL2> in(a.in0, a.in1, tr * a.in_stride);
+                        if (use_tma) {
+                            const F* sf = reinterpret_cast<const F*>(stage);
 #pragma unroll
-                        for (int i = 0; i < NB; ++i) {
-                            const int b = tb + i * T;
+                            for (int i = 0; i < NB; ++i) {
+                                const int b = tb + i * T;
 #pragma unroll
-                            for (int rho = 0; rho < G.R; ++rho) {
-                                const int pos = b + rho * (R / G.R);
-                                C x = in[U + pos * (N / R)];
-                                v[i * G.R + rho] = (Cfg::FIRST && !FWD) ? cswap(x) : x;
+                                for (int rho = 0; rho < G.R; ++rho) {
+                                    const int pos = b + rho * (R / G.R);
+                                    C x = kSoAIn ? cx<C>(sf[pos * UPC + u], sf[R * UPC + pos * UPC + u])
+                                                 : stage[pos * UPC + u];
+                                    v[i * G.R + rho] = (Cfg::FIRST && !FWD) ? cswap(x) : x;
+                                }
+                            }
+                            __syncthreads();  // staging fully read: refill it with the next item
+                            issue(item + gridDim.x);
+                        } else {
+                            const CxIn<F, IL2> in(a.in0, a.in1, tr * a.in_stride);
+#pragma unroll
+                            for (int i = 0; i < NB; ++i) {
+                                const int b = tb + i * T;
+#pragma unroll
+                                for (int rho = 0; rho < G.R; ++rho) {
+                                    const int pos = b + rho * (R / G.R);
+                                    C x = in[U + pos * (N / R)];
+                                    v[i * G.R + rho] = (Cfg::FIRST && !FWD) ? cswap(x) : x;
+                                }
                             }
                         }
                     } else {
