@@ -59,3 +59,23 @@ def test_python_mirror_rejects_bad_buffers():
         _real_arg(ro, 8, np.float32, "out", True)
     with pytest.raises(TypeError):
         Z.fft._prec(np.int32)
+
+
+def _build_dropin(tmp_path):
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    exe = tmp_path / "dropin"
+    cmd = ["g++", "-std=c++20", "-O2", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "dropin_example.cpp"),
+           "-L", os.path.join(ROOT, "zldsp_fft_b200", "lib"), "-lzlfft_cuda", "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_cpp_dropin_headers_compile_and_link(tmp_path):
+    """The reference's README usage compiles unchanged against the drop-in
+    headers (include/zldsp_fft_cuda/) and links against libzlfft_cuda.so."""
+    _build_dropin(tmp_path)

@@ -325,3 +325,24 @@ def test_multipass_chunks_strides_inplace(oracle):
     ref = oracle.cfft_port(x[:3], False)
     for i in range(3):
         assert np.array_equal(o[i * so: i * so + n], ref[i])
+
+
+def test_cpp_dropin_runs(tmp_path):
+    """The C++ drop-in classes (zldsp::fft::CFFT/RFFT over the C ABI) run the
+    reference's README example on the GPU and round-trip within tolerance."""
+    import os
+    import subprocess
+    from tests.test_capi_cpu import _build_dropin
+    exe = _build_dropin(tmp_path)
+    env = dict(os.environ)
+    libdir = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "zldsp_fft_b200", "lib")
+    env["LD_LIBRARY_PATH"] = libdir + ":" + env.get("LD_LIBRARY_PATH", "")
+    r = subprocess.run([str(exe)], capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "rfft0_throws=1" in r.stdout
+    n = 1024
+    i = np.arange(n, dtype=np.float32)
+    x = (np.sin(np.float32(0.1) * i) + 1j * np.cos(np.float32(0.3) * i)).astype(np.complex64)
+    X = np.fft.fft(x.astype(np.complex128))
+    got = r.stdout.split("X0=")[1].split()[0].split(",")
+    assert abs(float(got[0]) - X[0].real) < 1e-3 and abs(float(got[1]) - X[0].imag) < 1e-3
