@@ -175,6 +175,13 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* map, int x, i
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
         : "memory");
 }
+// Orders this thread's earlier generic-proxy shared-memory accesses before
+// later async-proxy (TMA) accesses of shared memory. Every thread that read a
+// staging buffer executes it before the barrier after which the buffer is
+// refilled by TMA; without it a read still in flight may observe the refill.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(

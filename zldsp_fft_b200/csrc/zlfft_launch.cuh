@@ -7,6 +7,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <stdlib.h>
 #include <string.h>
 
 #include "zlfft_pass.cuh"
@@ -119,7 +120,12 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
     PassArgs a = a_in;
     PassMaps maps;
     memset(&maps, 0, sizeof(maps));
-    a.tma = (a.tma && encode_pass_maps<F, P, PI, IL2>(a, maps)) ? 1 : 0;
+    // ZLFFT_PASS_TMA=0 selects direct loads (diagnostics and comparison).
+    static const bool tma_enabled = [] {
+        const char* e = getenv("ZLFFT_PASS_TMA");
+        return !(e && e[0] == '0');
+    }();
+    a.tma = (tma_enabled && a.tma && encode_pass_maps<F, P, PI, IL2>(a, maps)) ? 1 : 0;
     static const int blocks_per_sm = [kern]() {
         if (Cfg::SMEM > 48 * 1024)
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);

@@ -211,7 +211,8 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                                     v[i * G.R + rho] = (Cfg::FIRST && !FWD) ? cswap(x) : x;
                                 }
                             }
-                            __syncthreads();  // staging fully read: refill it with the next item
+                            fence_proxy_async_smem();  // reads of the staging buffer before its TMA refill
+                            __syncthreads();           // staging fully read: refill it with the next item
                             issue(item + gridDim.x);
                         } else {
                             const CxIn<F, IL2> in(a.in0, a.in1, tr * a.in_stride);

@@ -509,7 +509,8 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
                                         v[u * G.R + rho] = kFwd ? x : cswap(x);
                                     }
                                 }
-                                __syncthreads();  // staging fully read: refill it with the next tile
+                                fence_proxy_async_smem();  // reads of the staging buffer before its TMA refill
+                                __syncthreads();           // staging fully read: refill it with the next tile
                                 issue(tile + gridDim.x);
                             } else {
                                 constexpr int IL2 = kR2C ? (int)kAoS : IL;
