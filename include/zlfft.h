@@ -118,6 +118,35 @@ ZLFFT_API int zlfft_exec_host_batched(zlfft_plan plan, int op, int in_layout, in
 ZLFFT_API int zlfft_exec_device(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0, const void* in1,
                       void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, void* stream);
 
+/* As zlfft_exec_device, for callers that cannot allocate device memory when
+ * they run a transform: a real-time audio thread (an allocation can block
+ * for an unbounded time), work being captured into a CUDA graph (cudaMalloc
+ * is not allowed during capture), or a host whose device memory is all
+ * handed to its own pool. No reference counterpart: the reference allocates
+ * everything in its constructors.
+ *
+ * Orders 14 and up pass their intermediates through a scratch array built
+ * into the library (64 MiB of device memory, reserved on every GPU that loads
+ * the library and held until the process exits), instead of the plan's
+ * scratch that zlfft_exec_device allocates on first use. This call allocates
+ * nothing and creates no streams or events; orders <= 13 need no scratch and
+ * run exactly as in zlfft_exec_device. Results are identical to
+ * zlfft_exec_device's.
+ *  - Limit: one transform must fit one 32 MiB half of the array (FP32 order
+ *    <= 22, FP64 order <= 21); larger orders are rejected with
+ *    ZLFFT_ERR_UNSUPPORTED.
+ *  - The first call on each device looks up the array's device address
+ *    (cudaGetSymbolAddress), which may make the driver load the library's
+ *    device code; make that first call during set-up, before any stream
+ *    capture or real-time section.
+ *  - Every call shares the one array and leaves its contents behind (nothing
+ *    in it needs to start at zero). Calls whose work overlaps on the GPU
+ *    (different streams, or different plans at once) race on it: serialise
+ *    them, e.g. on one stream. */
+ZLFFT_API int zlfft_exec_device_noalloc(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0,
+                                        const void* in1, void* out0, void* out1, size_t batch, size_t in_stride,
+                                        size_t out_stride, void* stream);
+
 /* Number of CUDA kernels this plan has launched since the previous call
  * (diagnostics for benchmarks). */
 ZLFFT_API int zlfft_plan_take_launch_count(zlfft_plan plan, size_t* launches);

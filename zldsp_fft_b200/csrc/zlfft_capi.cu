@@ -487,6 +487,184 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     return ZLFFT_OK;
 }
 
+// ------------------------------------------------------------------ allocation-free execution
+// Some callers cannot allocate device memory at the moment they run a
+// transform: a real-time audio callback must not block on the allocator,
+// work recorded into a CUDA graph must not call cudaMalloc during capture,
+// and hosts that hand the whole device to a memory pool get no memory
+// outside it. Orders 14 and up need intermediate buffers between their
+// passes, which zlfft_exec_device allocates on first use. For those callers
+// the library carries its own scratch: one array in device memory, reserved
+// when the library's device code is loaded and held until the process exits.
+constexpr size_t kNoAllocScratchBytes = size_t{64} << 20;  // two halves of 32 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocSlot {
+    std::once_flag once;
+    void* ptr = nullptr;
+    cudaError_t err = cudaSuccess;
+};
+NoAllocSlot g_noalloc_slots[kNoAllocMaxDevices];
+
+// Device address of the array on `device`. In host code the array's name is
+// only a host-side stand-in, so the address is looked up with
+// cudaGetSymbolAddress, once per device, with that device current.
+int noalloc_scratch(int device, void** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(ZLFFT_ERR_INVALID_ARG, "device %d out of range", device);
+    NoAllocSlot& slot = g_noalloc_slots[device];
+    std::call_once(slot.once, [&]() {
+        DeviceGuard g(device);
+        slot.err = cudaGetSymbolAddress(&slot.ptr, g_noalloc_scratch);
+        if (slot.err != cudaSuccess) cudaGetLastError();
+    });
+    if (slot.err != cudaSuccess) return cuda_fail(slot.err, "cudaGetSymbolAddress(no-alloc scratch)");
+    *out = slot.ptr;
+    return ZLFFT_OK;
+}
+
+// The multi-pass orders with the built-in array as the pass intermediates:
+// chunks of transforms, one after another on the caller's stream (no helper
+// streams or events are created). Same kernels and arithmetic as
+// exec_multipass.
+int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layout, const zlfft::TileArgs& a,
+                           cudaStream_t st, const zlfft::LaunchCtx& ctx) {
+    const int P = p->cfft_order;
+    if (P < zlfft::kPassMinP || P > zlfft::kPassMaxP)
+        return fail(ZLFFT_ERR_UNSUPPORTED, "order %d is above the supported maximum", p->order);
+    const size_t cx = 2 * p->esize;
+    const long long n = 1LL << P;
+    const size_t half = kNoAllocScratchBytes / 2;
+    const size_t per = (size_t)n * cx;
+    if (per > half)
+        return fail(ZLFFT_ERR_UNSUPPORTED,
+                    "one transform needs %zu bytes of intermediate buffer; the allocation-free entry point holds "
+                    "%zu per buffer (order <= %d in this precision)",
+                    per, half, p->esize == 4 ? 22 : 21);
+    void* base = nullptr;
+    int rc = noalloc_scratch(p->device, &base);
+    if (rc) return rc;
+    const long long chunk = (long long)(half / per);
+    char* s0 = static_cast<char*>(base);
+    char* s1 = s0 + half;
+    const zlfft::PassTable& t = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
+    const auto& row = t.fn[P - zlfft::kPassMinP];
+    int np = 0;
+    while (np < zlfft::kMaxPasses && row[np][1][0][0]) ++np;
+    const bool fwd = (dop == zlfft::kC2CFwd || dop == zlfft::kR2CFwd || dop == zlfft::kR2CSqrMag);
+    const bool r2c = (dop == zlfft::kR2CFwd || dop == zlfft::kR2CSqrMag);
+    const bool c2r = (dop == zlfft::kC2RBwd);
+    const int il = r2c ? ZLFFT_AOS : in_layout;
+    const int ol = c2r ? ZLFFT_AOS : out_layout;
+    const size_t in_elem = (in_layout == ZLFFT_SOA && !r2c) ? p->esize : cx;
+    const size_t out_elem = (out_layout == ZLFFT_SOA && !c2r) ? p->esize : cx;
+    for (long long b0 = 0; b0 < a.batch; b0 += chunk) {
+        const long long nb = std::min<long long>(chunk, a.batch - b0);
+        const char* ui0 = static_cast<const char*>(a.in0) + b0 * a.in_stride * in_elem;
+        const char* ui1 = a.in1 ? static_cast<const char*>(a.in1) + b0 * a.in_stride * in_elem : nullptr;
+        char* uo0 = static_cast<char*>(a.out0) + b0 * a.out_stride * (dop == zlfft::kR2CSqrMag ? p->esize : out_elem);
+        char* uo1 = a.out1 ? static_cast<char*>(a.out1) + b0 * a.out_stride * out_elem : nullptr;
+        cudaError_t e;
+        const void* src0 = ui0;
+        const void* src1 = ui1;
+        long long src_stride = a.in_stride;
+        int src_layout = il;
+        if (c2r) {
+            e = p->prec == ZLFFT_F32 ? launch_pre<float>(p, in_layout, ui0, ui1, s0, nb, a.in_stride, st, ctx)
+                                     : launch_pre<double>(p, in_layout, ui0, ui1, s0, nb, a.in_stride, st, ctx);
+            if (e != cudaSuccess) return cuda_fail(e, "rfft pre-step launch");
+            src0 = s0;
+            src1 = nullptr;
+            src_stride = n;
+            src_layout = ZLFFT_AOS;
+        }
+        char* bufs[2] = {c2r ? s1 : s0, c2r ? s0 : s1};
+        for (int pi = 0; pi < np; ++pi) {
+            const bool last = (pi + 1 == np);
+            zlfft::PassArgs pa;
+            pa.in0 = src0;
+            pa.in1 = src1;
+            pa.in_stride = src_stride;
+            pa.batch = nb;
+            pa.tws = p->d_tws;
+            pa.err = p->d_err;
+            const size_t eb = (pi == 0 && src_layout == ZLFFT_SOA) ? p->esize : cx;
+            pa.tma = (aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
+                      (nb == 1 || ((size_t)src_stride * eb) % 16 == 0)) ? 1 : 0;
+            if (last && !r2c) {
+                pa.out0 = uo0;
+                pa.out1 = uo1;
+                pa.out_stride = a.out_stride;
+            } else {
+                pa.out0 = bufs[pi & 1];
+                pa.out1 = nullptr;
+                pa.out_stride = n;
+            }
+            const int li = pi == 0 ? src_layout : ZLFFT_AOS;
+            const int lo = (last && !r2c) ? ol : ZLFFT_AOS;
+            zlfft::PassLaunchFn fn = row[pi][fwd ? 1 : 0][li][lo];
+            if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no pass kernel for order %d", p->order);
+            e = fn(pa, st, ctx);
+            if (e != cudaSuccess) return cuda_fail(e, "pass launch");
+            src0 = pa.out0;
+            src1 = nullptr;
+            src_stride = n;
+        }
+        if (r2c) {
+            e = p->prec == ZLFFT_F32
+                    ? launch_split<float>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx)
+                    : launch_split<double>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx);
+            if (e != cudaSuccess) return cuda_fail(e, "rfft split launch");
+        }
+    }
+    return ZLFFT_OK;
+}
+
+// Argument checks of zlfft_exec_device, then the allocation-free dispatch.
+int exec_device_noalloc_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0,
+                             const void* in1, void* out0, void* out1, size_t batch, size_t in_stride,
+                             size_t out_stride, cudaStream_t stream) {
+    if (p->cfft_order <= zlfft::kTileMaxP)  // single-CTA orders use no scratch at all
+        return exec_device_impl(p, op, in_layout, out_layout, in0, in1, out0, out1, batch, in_stride, out_stride,
+                                stream);
+    int rc = validate_op(p, op, in_layout, out_layout);
+    if (rc) return rc;
+    const Extents ex = extents(p, op);
+    const bool in_soa = ex.in_complex && in_layout == ZLFFT_SOA;
+    const bool out_soa = ex.out_complex && out_layout == ZLFFT_SOA;
+    if (!in0 || (in_soa && !in1)) return fail(ZLFFT_ERR_INVALID_ARG, "null input pointer");
+    if (!out0 || (out_soa && !out1)) return fail(ZLFFT_ERR_INVALID_ARG, "null output pointer");
+    if (in_stride == 0) in_stride = ex.in_elems;
+    if (out_stride == 0) out_stride = ex.out_elems;
+    if (batch > 1 && (in_stride < ex.in_elems || out_stride < ex.out_elems))
+        return fail(ZLFFT_ERR_INVALID_ARG, "stride smaller than one transform");
+    const size_t pair = 2 * p->esize;
+    const bool in_pairs = ex.in_complex ? !in_soa : (op != ZLFFT_BACKWARD);
+    const bool out_pairs = ex.out_complex ? !out_soa : (p->kind == ZLFFT_R2C && op == ZLFFT_BACKWARD);
+    if (in_pairs && !aligned(in0, pair)) return fail(ZLFFT_ERR_ALIGNMENT, "input must be %zu-byte aligned", pair);
+    if (out_pairs && !aligned(out0, pair)) return fail(ZLFFT_ERR_ALIGNMENT, "output must be %zu-byte aligned", pair);
+    if (!aligned(in0, p->esize) || (in1 && !aligned(in1, p->esize)) || !aligned(out0, p->esize) ||
+        (out1 && !aligned(out1, p->esize)))
+        return fail(ZLFFT_ERR_ALIGNMENT, "buffers must be aligned to the element type");
+    if (!ex.in_complex && (in_stride % 2)) return fail(ZLFFT_ERR_INVALID_ARG, "RFFT real input stride must be even");
+    if (p->kind == ZLFFT_R2C && op == ZLFFT_BACKWARD && (out_stride % 2))
+        return fail(ZLFFT_ERR_INVALID_ARG, "RFFT real output stride must be even");
+    if (p->kind == ZLFFT_C2C && in0 == out0 && in_layout != out_layout)
+        return fail(ZLFFT_ERR_INVALID_ARG, "in-place transform needs the same layout on both sides");
+    if (batch == 0) return ZLFFT_OK;
+    zlfft::TileArgs a{};
+    a.in0 = in0;
+    a.in1 = in_soa ? in1 : nullptr;
+    a.out0 = out0;
+    a.out1 = out_soa ? out1 : nullptr;
+    a.batch = (long long)batch;
+    a.in_stride = (long long)(ex.in_complex ? in_stride : in_stride / 2);
+    a.out_stride = (long long)((ex.out_complex || op == ZLFFT_FORWARD_SQR_MAG) ? out_stride : out_stride / 2);
+    zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
+    DeviceGuard g(p->device);
+    return exec_multipass_noalloc(p, device_op_code(p, op), in_layout, out_layout, a, stream, ctx);
+}
+
 int ensure_staging(zlfft_plan_s* p, size_t in_bytes, size_t out_bytes) {
     if (in_bytes > p->stage_in_bytes) {
         if (p->h_in) cudaFreeHost(p->h_in);
@@ -737,6 +915,14 @@ int zlfft_exec_device(zlfft_plan plan, int op, int in_layout, int out_layout, co
     if (!plan) return fail(ZLFFT_ERR_INVALID_ARG, "null plan");
     return exec_device_impl(plan, op, in_layout, out_layout, in0, in1, out0, out1, batch, in_stride, out_stride,
                             static_cast<cudaStream_t>(stream));
+}
+
+int zlfft_exec_device_noalloc(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0,
+                              const void* in1, void* out0, void* out1, size_t batch, size_t in_stride,
+                              size_t out_stride, void* stream) {
+    if (!plan) return fail(ZLFFT_ERR_INVALID_ARG, "null plan");
+    return exec_device_noalloc_impl(plan, op, in_layout, out_layout, in0, in1, out0, out1, batch, in_stride,
+                                    out_stride, static_cast<cudaStream_t>(stream));
 }
 
 int zlfft_plan_take_launch_count(zlfft_plan plan, size_t* launches) {
