@@ -264,6 +264,7 @@ class Cfft2G:
     input (batch 16384 / 4096 / 256); one step = forward then backward of all
     three (plain FP32 form). re, im ~ U[-1, 1), seed 1003."""
     name = "cfft2g"
+    l2 = "each op reads 2 GiB and writes 2 GiB, > 16x L2 (no L2 flush needed)"
     desc = "CFFT<float> orders 14/16/20 x 2 GiB complex64 each (batch 16384/4096/256), forward + backward"
     orders = (14, 16, 20)
     total = 1 << 28  # complex elements per order (2 GiB)
@@ -360,7 +361,154 @@ class Cfft2G:
         return nbytes, dt
 
 
-WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G}
+class Mixed:
+    """Mixed-order batch: 20,000 transforms, order ~ U{6..16}, half CFFT<float>
+    forward AoS and half RFFT<float> forward AoS, lengths and data from seed
+    1004 (entries ~ U[-1, 1)). Inputs are packed back to back in one device
+    buffer and outputs in another (each transform 256-byte aligned), so the
+    batch is addressed through per-transform pointers. One step runs the whole
+    batch with the persistent schedule replayed from a CUDA graph; the
+    per-order launch loop and the un-captured persistent schedule are timed
+    beside it."""
+    name = "mixed"
+    l2 = "each step reads 1.42 GB and writes 1.42 GB, > 10x L2 (no L2 flush needed)"
+    desc = ("mixed batch: 20,000 transforms, order U{6..16}, 50% CFFT<float> forward AoS / 50% RFFT<float> "
+            "forward AoS, seed 1004; persistent schedule replayed from a CUDA graph")
+    count = 20000
+    dtype = "f32"
+
+    def __init__(self):
+        rng = np.random.default_rng(1004)
+        self.orders = rng.integers(6, 17, self.count)
+        self.is_c = rng.random(self.count) < 0.5
+        n = (1 << self.orders).astype(np.int64)
+        self.in_sz = np.where(self.is_c, 8 * n, 4 * n)
+        self.out_sz = np.where(self.is_c, 8 * n, 8 * (n // 2 + 1))
+        up = lambda v: (v + 255) // 256 * 256  # noqa: E731
+        self.in_off = np.concatenate([[0], np.cumsum(up(self.in_sz))[:-1]])
+        self.out_off = np.concatenate([[0], np.cumsum(up(self.out_sz))[:-1]])
+        self.in_total = int(up(self.in_sz).sum())
+        self.out_total = int(up(self.out_sz).sum())
+        self.bytes_per_step = int(self.in_sz.sum() + self.out_sz.sum())
+        self.op_bytes = {"mixed_graph": self.bytes_per_step}
+        self.dominant = "mixed_graph"
+        self.batch = self.count
+        self.host_in = None
+
+    def setup(self, device):
+        import torch
+        import zldsp_fft_b200 as Z
+        self.Z = Z
+        g = torch.Generator(device=device)
+        g.manual_seed(1004)
+        self.A = (torch.rand(self.in_total // 4, generator=g, device=device) * 2 - 1).contiguous()
+        self.B = torch.zeros(self.out_total // 4, dtype=torch.float32, device=device)
+        a, b = self.A.data_ptr(), self.B.data_ptr()
+        descs = [(Z.C2C if c else Z.R2C, int(o), Z.FORWARD, a + int(io), b + int(oo))
+                 for c, o, io, oo in zip(self.is_c, self.orders, self.in_off, self.out_off)]
+        self.mb = Z.MixedBatch(descs, np.float32, device=device)
+        torch.cuda.synchronize(device)
+
+    def ops(self, step):
+        Z = self.Z
+        return [("mixed_graph", lambda st: self.mb.run(Z.SCHED_GRAPH, st))]
+
+    def take_launches(self):
+        return self.mb.take_launch_count()
+
+    def compare(self, stream, reps):
+        """GB/s and launches per step of every schedule; max relative-L2 error
+        of a sample (two transforms per (kind, order)) against numpy FP64."""
+        import torch
+        Z = self.Z
+        out = {}
+        for name, sched in (("per_order_loop", Z.SCHED_PER_ORDER), ("persistent", Z.SCHED_PERSISTENT),
+                            ("graph", Z.SCHED_GRAPH)):
+            for _ in range(2):
+                self.mb.run(sched, stream.cuda_stream)
+            torch.cuda.synchronize()
+            self.mb.take_launch_count()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                self.mb.run(sched, stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            out[name] = {"gbs": round(self.bytes_per_step / (ms / 1e3) / 1e9, 1), "ms": round(ms, 4),
+                         "launches": self.mb.take_launch_count() // reps}
+        A, B = self.A.cpu().numpy(), self.B.cpu().numpy()
+        worst, seen = 0.0, {}
+        for i in range(self.count):
+            key = (bool(self.is_c[i]), int(self.orders[i]))
+            if seen.get(key, 0) >= 2:
+                continue
+            seen[key] = seen.get(key, 0) + 1
+            n = 1 << key[1]
+            io, oo = int(self.in_off[i]) // 4, int(self.out_off[i]) // 4
+            if key[0]:
+                x = A[io:io + 2 * n].astype(np.float64).view(np.complex128)
+                ref = np.fft.fft(x)
+                y = B[oo:oo + 2 * n].astype(np.float64).view(np.complex128)
+            else:
+                ref = np.fft.rfft(A[io:io + n].astype(np.float64))
+                y = B[oo:oo + 2 * (n // 2 + 1)].astype(np.float64).view(np.complex128)
+            worst = max(worst, float(np.linalg.norm(y - ref) / np.linalg.norm(ref)))
+        out["max_rel_l2_vs_fp64"] = worst
+        out["tolerance_order16"] = 4 * 16 * 2.0 ** -24
+        return out
+
+    def cpu_sample_desc(self, frames):
+        return f"the first {frames} of the 20,000 transforms, grouped by (kind, order), median of 3"
+
+    def setup_e2e(self):
+        import torch
+        self.hA = self.A.cpu().pin_memory()
+        self.hB = torch.empty_like(self.B, device="cpu").pin_memory()
+        self.e2e_h2d = self.hA.numel() * 4
+        self.e2e_d2h = self.hB.numel() * 4
+
+    def e2e_step(self):
+        import torch
+        st = torch.cuda.current_stream()
+        self.A.copy_(self.hA, non_blocking=True)
+        self.mb.run(self.Z.SCHED_GRAPH, st.cuda_stream)
+        self.hB.copy_(self.B, non_blocking=True)
+        st.synchronize()
+
+    def cpu_run(self, frames, threads, kind):
+        """The first `frames` transforms, one reference object per (kind, order)."""
+        from oracle import oracle as O
+        rng = np.random.default_rng(1004)
+        frames = min(frames, self.count)
+        nbytes, dt = 0.0, 0.0
+        groups = {}
+        for i in range(frames):
+            groups.setdefault((bool(self.is_c[i]), int(self.orders[i])), []).append(i)
+        for (is_c, o), idx in sorted(groups.items()):
+            n, cnt = 1 << o, len(idx)
+            if is_c:
+                x = (rng.uniform(-1, 1, (cnt, n)) + 1j * rng.uniform(-1, 1, (cnt, n))).astype(np.complex64)
+            else:
+                x = rng.uniform(-1, 1, (cnt, n)).astype(np.float32)
+            if kind == "reference":
+                plan = O.RefPlan("c2c" if is_c else "r2c", o, "f32", threads)
+                t0 = time.perf_counter()
+                if is_c:
+                    plan.cfft(x, True, out=np.empty_like(x))
+                else:
+                    plan.rfft_forward(x, O.AOS, out=np.empty((cnt, n // 2 + 1), np.complex64))
+                dt += time.perf_counter() - t0
+                plan.close()
+            else:
+                t0 = time.perf_counter()
+                O.cfft_port(x, True) if is_c else O.rfft_forward_port(x)
+                dt += time.perf_counter() - t0
+            nbytes += float(self.in_sz[idx].sum() + self.out_sz[idx].sum())
+        return nbytes, dt
+
+
+WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G, "mixed": Mixed}
 
 
 # ------------------------------------------------------------------ CPU baseline
@@ -498,6 +646,7 @@ def run_ours(args, wl_cls):
         e2e_s = float(t.item())
     e2e_val = wl.bytes_per_step * e2e_steps * world / e2e_s / 1e9
     wl.take_launches()
+    schedules = wl.compare(stream, max(3, min(args.steps, 10))) if hasattr(wl, "compare") else None
 
     peak, peak_kind = measured_hbm_peak()
     dom = wl.dominant
@@ -508,7 +657,7 @@ def run_ours(args, wl_cls):
         "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic",
         "config": {"workload": wl.desc, "form": "plain FP32 (reference's Stockham radix-4/8 DIT, CUDA cores)",
-                   "l2": "rotating input/output sets, each step > 2x L2 (no L2 flush needed)",
+                   "l2": getattr(wl, "l2", "rotating input/output sets, each step > 2x L2 (no L2 flush needed)"),
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
@@ -520,6 +669,8 @@ def run_ours(args, wl_cls):
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
+    if schedules is not None:
+        line["schedules"] = schedules
     if rank == 0:
         if world == 1 and not args.no_cpu:
             try:

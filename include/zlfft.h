@@ -171,6 +171,59 @@ ZLFFT_API int zlfft_plan_device_status(zlfft_plan plan, int* status);
  * as designed). The GPU context stays usable. No reference counterpart. */
 ZLFFT_API int zlfft_selftest_bounded_wait(int device, int* status);
 
+/* ---------------------------------------------------------------- mixed batches
+ * Many transforms of different orders and kinds in one call. No reference
+ * counterpart: the reference runs one CFFT<F>/RFFT<F> object per length
+ * (src/zldsp_fft_cfft.hpp:19, src/zldsp_fft_rfft.hpp:24), so a host program
+ * with transforms of several lengths calls forward()/backward() on several
+ * objects one after another; here the whole set is one descriptor list. */
+
+/* One transform of a mixed batch. Buffers are device pointers, AoS layout
+ * (interleaved complex; RFFT real sides are plain arrays of F), aligned to
+ * 2 * sizeof(F); the real output of forward_sqr_mag to sizeof(F). */
+typedef struct zlfft_desc {
+    int kind;        /* ZLFFT_C2C or ZLFFT_R2C */
+    int precision;   /* ZLFFT_F32 or ZLFFT_F64 */
+    int order;       /* log2 of the transform length (RFFT: of the real length) */
+    int op;          /* ZLFFT_FORWARD, ZLFFT_BACKWARD, ZLFFT_FORWARD_SQR_MAG (RFFT) */
+    const void* in;  /* input of this transform */
+    void* out;       /* output of this transform; may equal `in` for C2C */
+} zlfft_desc;
+
+typedef struct zlfft_mixed_s* zlfft_mixed;
+
+/* schedules of zlfft_mixed_exec */
+#define ZLFFT_SCHED_PER_ORDER 0  /* one batched launch per (kind, order, op) group, in a loop */
+#define ZLFFT_SCHED_PERSISTENT 1 /* complex orders <= 11 of every group in one persistent launch */
+#define ZLFFT_SCHED_GRAPH 2      /* the persistent schedule recorded once into a CUDA graph, replayed */
+
+/* Prepare a mixed batch of n descriptors on `device` (-1: current): plans per
+ * (kind, precision, order), the gathered per-transform pointer arrays, the
+ * persistent kernel's work list (tiles sorted longest first) and the
+ * multi-pass intermediates, all allocated here, so that zlfft_mixed_exec
+ * allocates nothing and may be recorded into a CUDA graph. The descriptors
+ * are copied; the buffers they point to are used by every exec. */
+ZLFFT_API int zlfft_mixed_create(zlfft_mixed* mixed, const zlfft_desc* descs, size_t n, int device);
+
+/* Run every transform of the batch on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream), asynchronously, with the given ZLFFT_SCHED_*.
+ * Results are identical across schedules. Calls on one mixed object must not
+ * overlap on the GPU (they share its work-list counter and intermediates). */
+ZLFFT_API int zlfft_mixed_exec(zlfft_mixed mixed, int schedule, void* stream);
+
+/* Number of CUDA kernels the batch's executions have launched since the
+ * previous call (a graph replay counts the kernels it contains). */
+ZLFFT_API int zlfft_mixed_take_launch_count(zlfft_mixed mixed, size_t* launches);
+
+/* zlfft_plan_device_status over every plan of the batch. */
+ZLFFT_API int zlfft_mixed_device_status(zlfft_mixed mixed, int* status);
+
+ZLFFT_API int zlfft_mixed_destroy(zlfft_mixed mixed);
+
+/* One-shot form: create, run with ZLFFT_SCHED_PERSISTENT on `stream`,
+ * synchronise the stream, destroy. */
+ZLFFT_API int zlfft_exec_mixed_device(const zlfft_desc* descs, size_t n, void* stream);
+
 /* Message of the calling thread's last failure ("" if none). */
 ZLFFT_API const char* zlfft_last_error(void);
 

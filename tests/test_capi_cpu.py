@@ -44,6 +44,33 @@ def test_invalid_arguments_rejected_without_cuda():
     assert lib.zlfft_plan_get_size(None, ctypes.byref(sz)) == C.ERR_INVALID_ARG
 
 
+def test_mixed_batch_descriptors_rejected_without_cuda():
+    """zlfft_mixed_create checks every descriptor before it touches CUDA."""
+    lib = C.lib()
+    h = ctypes.c_void_p()
+    ok = dict(kind=C.C2C, precision=C.F32, order=10, op=C.FORWARD, in_=4096, out=8192)
+
+    def one(**kw):
+        d = dict(ok)
+        d.update(kw)
+        arr = (C.Desc * 2)(C.Desc(**ok), C.Desc(**d))
+        return lib.zlfft_mixed_create(ctypes.byref(h), arr, 2, -1)
+
+    assert lib.zlfft_mixed_create(None, None, 0, -1) == C.ERR_INVALID_ARG
+    assert lib.zlfft_mixed_create(ctypes.byref(h), None, 3, -1) == C.ERR_INVALID_ARG
+    assert one(kind=5) == C.ERR_INVALID_ARG and "descriptor 1" in C.last_error()
+    assert one(precision=9) == C.ERR_INVALID_ARG
+    assert one(order=25) == C.ERR_UNSUPPORTED
+    assert one(kind=C.R2C, order=0) == C.ERR_UNSUPPORTED  # RFFT order 0 has no inner CFFT
+    assert one(op=7) == C.ERR_INVALID_ARG
+    assert one(op=C.FORWARD_SQR_MAG) == C.ERR_INVALID_ARG  # an RFFT operation
+    assert one(in_=None) == C.ERR_INVALID_ARG
+    assert one(out=8196) == C.ERR_ALIGNMENT  # complex64 output needs 8-byte alignment
+    assert one(precision=C.F64, in_=4104) == C.ERR_ALIGNMENT  # complex128 needs 16
+    assert lib.zlfft_mixed_exec(None, 1, None) == C.ERR_INVALID_ARG
+    assert lib.zlfft_mixed_destroy(None) == C.OK
+
+
 def test_python_mirror_rejects_bad_buffers():
     from zldsp_fft_b200.fft import _complex_arg, _real_arg
     import numpy as np

@@ -9,10 +9,11 @@ Layers:
 """
 from . import _capi
 from ._capi import (AOS, BACKWARD, C2C, F32, F64, FORWARD, FORWARD_SQR_MAG, MODE_PLAIN, MODE_TC_BF16,
-                    MODE_TC_FP16, MODE_TC_TF32, R2C, SOA, ZlfftError)
-from .fft import CFFT, RFFT, Plan
+                    MODE_TC_FP16, MODE_TC_TF32, R2C, SCHED_GRAPH, SCHED_PER_ORDER, SCHED_PERSISTENT, SOA,
+                    ZlfftError)
+from .fft import CFFT, RFFT, MixedBatch, Plan
 
 __all__ = [
-    "CFFT", "RFFT", "Plan", "ZlfftError", "AOS", "SOA", "C2C", "R2C", "F32", "F64", "FORWARD", "BACKWARD",
+    "CFFT", "RFFT", "Plan", "MixedBatch", "ZlfftError", "AOS", "SOA", "C2C", "R2C", "F32", "F64", "FORWARD", "BACKWARD",
     "FORWARD_SQR_MAG", "MODE_PLAIN", "MODE_TC_FP16", "MODE_TC_BF16", "MODE_TC_TF32",
 ]

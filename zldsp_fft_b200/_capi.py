@@ -27,6 +27,14 @@ F32, F64 = 0, 1
 AOS, SOA = 0, 1
 FORWARD, BACKWARD, FORWARD_SQR_MAG = 0, 1, 2
 MODE_PLAIN, MODE_TC_FP16, MODE_TC_BF16, MODE_TC_TF32 = 0, 1, 2, 3
+SCHED_PER_ORDER, SCHED_PERSISTENT, SCHED_GRAPH = 0, 1, 2
+
+
+class Desc(ctypes.Structure):
+    """zlfft_desc: one transform of a mixed batch (device pointers)."""
+    _fields_ = [("kind", ctypes.c_int), ("precision", ctypes.c_int), ("order", ctypes.c_int), ("op", ctypes.c_int),
+                ("in_", ctypes.c_void_p), ("out", ctypes.c_void_p)]
+
 
 # every symbol include/zlfft.h declares
 EXPORTS = (
@@ -42,6 +50,12 @@ EXPORTS = (
     "zlfft_plan_copy_twiddles",
     "zlfft_plan_device_status",
     "zlfft_selftest_bounded_wait",
+    "zlfft_mixed_create",
+    "zlfft_mixed_exec",
+    "zlfft_mixed_take_launch_count",
+    "zlfft_mixed_device_status",
+    "zlfft_mixed_destroy",
+    "zlfft_exec_mixed_device",
     "zlfft_last_error",
     "zlfft_version",
 )
@@ -82,6 +96,12 @@ def lib() -> ctypes.CDLL:
         L.zlfft_plan_copy_twiddles.argtypes = [vp, vp, sz, ctypes.POINTER(sz)]
         L.zlfft_plan_device_status.argtypes = [vp, ctypes.POINTER(i)]
         L.zlfft_selftest_bounded_wait.argtypes = [i, ctypes.POINTER(i)]
+        L.zlfft_mixed_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(Desc), sz, i]
+        L.zlfft_mixed_exec.argtypes = [vp, i, vp]
+        L.zlfft_mixed_take_launch_count.argtypes = [vp, ctypes.POINTER(sz)]
+        L.zlfft_mixed_device_status.argtypes = [vp, ctypes.POINTER(i)]
+        L.zlfft_mixed_destroy.argtypes = [vp]
+        L.zlfft_exec_mixed_device.argtypes = [ctypes.POINTER(Desc), sz, vp]
         L.zlfft_last_error.restype = ctypes.c_char_p
         L.zlfft_last_error.argtypes = []
         L.zlfft_version.restype = ctypes.c_char_p

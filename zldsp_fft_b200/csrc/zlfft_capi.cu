@@ -11,11 +11,15 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
+#include <vector>
 
 #include "../../include/zlfft.h"
 #include "zlfft_launch.cuh"
+#include "zlfft_mixed.cuh"
 
 namespace {
 
@@ -115,7 +119,11 @@ struct TablesHolder {
     zlfft::TileTable f64{};
     zlfft::PassTable p32{};
     zlfft::PassTable p64{};
+    zlfft::GatherTable g32{};
+    zlfft::GatherTable g64{};
     TablesHolder() {
+        zlfft::fill_gather_f32(g32);
+        zlfft::fill_gather_f64(g64);
         zlfft::fill_tile_c2c_f32(f32);
         zlfft::fill_tile_r2c_f32(f32);
         zlfft::fill_tile_c2c_f64(f64);
@@ -268,7 +276,8 @@ int ensure_scratch(zlfft_plan_s* p) {
 
 template <typename F>
 cudaError_t launch_split(const zlfft_plan_s* p, int dop, int out_layout, const void* z, void* o0, void* o1,
-                         long long batch, long long out_stride, cudaStream_t st, const zlfft::LaunchCtx& ctx) {
+                         long long batch, long long out_stride, cudaStream_t st, const zlfft::LaunchCtx& ctx,
+                         void* const* go0 = nullptr, void* const* go1 = nullptr) {
     using C = zlfft::Cx<F>;
     const int M = 1 << p->cfft_order;
     const long long total = (long long)(M / 2 + 1) * batch;
@@ -276,27 +285,28 @@ cudaError_t launch_split(const zlfft_plan_s* p, int dop, int out_layout, const v
     const C* zc = static_cast<const C*>(z);
     const C* rw = static_cast<const C*>(p->d_rw);
     if (dop == zlfft::kR2CSqrMag)
-        zlfft::rfft_split_kernel<F, zlfft::kR2CSqrMag, zlfft::kAoS><<<grid, 256, 0, st>>>(zc, o0, o1, rw, M, batch, M, out_stride);
+        zlfft::rfft_split_kernel<F, zlfft::kR2CSqrMag, zlfft::kAoS><<<grid, 256, 0, st>>>(zc, o0, o1, rw, M, batch, M, out_stride, go0, go1);
     else if (out_layout == ZLFFT_AOS)
-        zlfft::rfft_split_kernel<F, zlfft::kR2CFwd, zlfft::kAoS><<<grid, 256, 0, st>>>(zc, o0, o1, rw, M, batch, M, out_stride);
+        zlfft::rfft_split_kernel<F, zlfft::kR2CFwd, zlfft::kAoS><<<grid, 256, 0, st>>>(zc, o0, o1, rw, M, batch, M, out_stride, go0, go1);
     else
-        zlfft::rfft_split_kernel<F, zlfft::kR2CFwd, zlfft::kSoA><<<grid, 256, 0, st>>>(zc, o0, o1, rw, M, batch, M, out_stride);
+        zlfft::rfft_split_kernel<F, zlfft::kR2CFwd, zlfft::kSoA><<<grid, 256, 0, st>>>(zc, o0, o1, rw, M, batch, M, out_stride, go0, go1);
     if (ctx.launches) ++*ctx.launches;
     return cudaGetLastError();
 }
 
 template <typename F>
 cudaError_t launch_pre(const zlfft_plan_s* p, int in_layout, const void* i0, const void* i1, void* z, long long batch,
-                       long long in_stride, cudaStream_t st, const zlfft::LaunchCtx& ctx) {
+                       long long in_stride, cudaStream_t st, const zlfft::LaunchCtx& ctx,
+                       const void* const* gi0 = nullptr, const void* const* gi1 = nullptr) {
     using C = zlfft::Cx<F>;
     const int M = 1 << p->cfft_order;
     const long long total = (long long)(M / 2 + 1) * batch;
     const unsigned grid = (unsigned)std::min<long long>((total + 255) / 256, (long long)p->num_sms * 16);
     const C* rw = static_cast<const C*>(p->d_rw);
     if (in_layout == ZLFFT_AOS)
-        zlfft::rfft_pre_kernel<F, zlfft::kAoS><<<grid, 256, 0, st>>>(i0, i1, static_cast<C*>(z), rw, M, batch, in_stride, M);
+        zlfft::rfft_pre_kernel<F, zlfft::kAoS><<<grid, 256, 0, st>>>(i0, i1, static_cast<C*>(z), rw, M, batch, in_stride, M, gi0, gi1);
     else
-        zlfft::rfft_pre_kernel<F, zlfft::kSoA><<<grid, 256, 0, st>>>(i0, i1, static_cast<C*>(z), rw, M, batch, in_stride, M);
+        zlfft::rfft_pre_kernel<F, zlfft::kSoA><<<grid, 256, 0, st>>>(i0, i1, static_cast<C*>(z), rw, M, batch, in_stride, M, gi0, gi1);
     if (ctx.launches) ++*ctx.launches;
     return cudaGetLastError();
 }
@@ -340,16 +350,22 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
     }
     const cudaStream_t caller = st;
     const size_t quarter = p->scratch_bytes / 4;
+    const bool gather = a.gin0 != nullptr;
     for (long long b0 = 0, ci = 0; b0 < a.batch; b0 += (long long)p->chunk, ++ci) {
         const long long nb = std::min<long long>((long long)p->chunk, a.batch - b0);
         if (fork) st = p->lanes[ci & 1];
         s0 = static_cast<char*>(p->d_scratch) + (size_t)(fork ? (ci & 1) : 0) * 2 * quarter;
         s1 = s0 + quarter;
-        // this chunk's user buffers
-        const char* ui0 = static_cast<const char*>(a.in0) + b0 * a.in_stride * in_elem;
-        const char* ui1 = a.in1 ? static_cast<const char*>(a.in1) + b0 * a.in_stride * in_elem : nullptr;
-        char* uo0 = static_cast<char*>(a.out0) + b0 * a.out_stride * (dop == zlfft::kR2CSqrMag ? p->esize : out_elem);
-        char* uo1 = a.out1 ? static_cast<char*>(a.out1) + b0 * a.out_stride * out_elem : nullptr;
+        // this chunk's user buffers: base + stride, or the chunk's slice of the gather arrays
+        const char* ui0 = gather ? nullptr : static_cast<const char*>(a.in0) + b0 * a.in_stride * in_elem;
+        const char* ui1 = (!gather && a.in1) ? static_cast<const char*>(a.in1) + b0 * a.in_stride * in_elem : nullptr;
+        char* uo0 = gather ? nullptr
+                           : static_cast<char*>(a.out0) + b0 * a.out_stride * (dop == zlfft::kR2CSqrMag ? p->esize : out_elem);
+        char* uo1 = (!gather && a.out1) ? static_cast<char*>(a.out1) + b0 * a.out_stride * out_elem : nullptr;
+        const void* const* gi0 = gather ? a.gin0 + b0 : nullptr;
+        const void* const* gi1 = (gather && a.gin1) ? a.gin1 + b0 : nullptr;
+        void* const* go0 = gather ? a.gout0 + b0 : nullptr;
+        void* const* go1 = (gather && a.gout1) ? a.gout1 + b0 : nullptr;
         cudaError_t e;
         // CFFT source/destination for this chunk
         const void* src0 = ui0;
@@ -357,8 +373,8 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
         long long src_stride = a.in_stride;
         int src_layout = il;
         if (c2r) {
-            e = p->prec == ZLFFT_F32 ? launch_pre<float>(p, in_layout, ui0, ui1, s0, nb, a.in_stride, st, ctx)
-                                     : launch_pre<double>(p, in_layout, ui0, ui1, s0, nb, a.in_stride, st, ctx);
+            e = p->prec == ZLFFT_F32 ? launch_pre<float>(p, in_layout, ui0, ui1, s0, nb, a.in_stride, st, ctx, gi0, gi1)
+                                     : launch_pre<double>(p, in_layout, ui0, ui1, s0, nb, a.in_stride, st, ctx, gi0, gi1);
             if (e != cudaSuccess) return cuda_fail(e, "rfft pre-step launch");
             src0 = s0;
             src1 = nullptr;
@@ -368,23 +384,30 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
         char* bufs[2] = {c2r ? s1 : s0, c2r ? s0 : s1};
         for (int pi = 0; pi < np; ++pi) {
             const bool last = (pi + 1 == np);
-            zlfft::PassArgs pa;
+            const bool gfirst = gather && pi == 0 && !c2r;  // the first pass reads gathered inputs
+            zlfft::PassArgs pa{};
             pa.in0 = src0;
             pa.in1 = src1;
             pa.in_stride = src_stride;
             pa.batch = nb;
             pa.tws = p->d_tws;
             pa.err = p->d_err;
+            if (gfirst) {
+                pa.gin0 = gi0;
+                pa.gin1 = gi1;
+            }
             {
                 // bulk-copy rows need 16-byte aligned sources (bases and transform stride)
                 const size_t eb = (pi == 0 && src_layout == ZLFFT_SOA) ? p->esize : cx;
-                pa.tma = (aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
+                pa.tma = (!gfirst && aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
                           (nb == 1 || ((size_t)src_stride * eb) % 16 == 0)) ? 1 : 0;
             }
             if (last && !r2c) {
                 pa.out0 = uo0;
                 pa.out1 = uo1;
                 pa.out_stride = a.out_stride;
+                pa.gout0 = go0;
+                pa.gout1 = go1;
             } else {
                 pa.out0 = bufs[pi & 1];
                 pa.out1 = nullptr;
@@ -402,8 +425,8 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
         }
         if (r2c) {
             e = p->prec == ZLFFT_F32
-                    ? launch_split<float>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx)
-                    : launch_split<double>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx);
+                    ? launch_split<float>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx, go0, go1)
+                    : launch_split<double>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx, go0, go1);
             if (e != cudaSuccess) return cuda_fail(e, "rfft split launch");
         }
     }
@@ -448,7 +471,7 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
         return fail(ZLFFT_ERR_INVALID_ARG, "in-place transform needs the same layout on both sides");
     if (batch == 0) return ZLFFT_OK;
 
-    zlfft::TileArgs a;
+    zlfft::TileArgs a{};
     a.in0 = in0;
     a.in1 = in_soa ? in1 : nullptr;
     a.out0 = out0;
@@ -581,7 +604,7 @@ int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layo
         char* bufs[2] = {c2r ? s1 : s0, c2r ? s0 : s1};
         for (int pi = 0; pi < np; ++pi) {
             const bool last = (pi + 1 == np);
-            zlfft::PassArgs pa;
+            zlfft::PassArgs pa{};
             pa.in0 = src0;
             pa.in1 = src1;
             pa.in_stride = src_stride;
@@ -774,6 +797,308 @@ int exec_host_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const
     return ZLFFT_OK;
 }
 
+
+// ------------------------------------------------------------------ mixed batches
+// A mixed batch is sorted on the host into groups of one (precision, kind,
+// order, operation); each group's transforms are addressed through gathered
+// pointer arrays (transform t of the group reads gin[t], writes gout[t]).
+// Groups whose complex order fits a 128-thread tile (2..11) become tiles of
+// one persistent launch per precision (zlfft_mixed.cuh); the others run as
+// gathered batched launches of the tile kernel (orders 0, 1, 12, 13) or of
+// the multi-pass pipeline (14 and up), largest first.
+struct MixedGroupHost {
+    zlfft_plan plan;
+    int prec;
+    int dop;     // device operation code
+    int P;       // complex order
+    size_t first;  // offset of the group in the gather arrays
+    size_t count;
+};
+
+}  // namespace
+
+struct zlfft_mixed_s {
+    int device = 0;
+    int num_sms = 0;
+    std::vector<zlfft_plan> plans;
+    std::vector<MixedGroupHost> groups;  // sorted by complex order, largest first
+    void* d_mem = nullptr;               // gather arrays, group records, work lists, counters
+    const void** d_gin = nullptr;
+    void** d_gout = nullptr;
+    zlfft::MixedGroup* d_mgroups[2] = {nullptr, nullptr};  // per precision
+    zlfft::MixedItem* d_items[2] = {nullptr, nullptr};
+    int n_items[2] = {0, 0};
+    int* d_counter = nullptr;  // one work-list counter per precision
+    cudaStream_t cap_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    size_t graph_launches = 0;  // kernels recorded in the graph
+    size_t launches = 0;
+    std::mutex mu;
+};
+
+namespace {
+
+void mixed_release(zlfft_mixed m) {
+    if (!m) return;
+    {
+        DeviceGuard g(m->device);
+        if (m->graph_exec) cudaGraphExecDestroy(m->graph_exec);
+        if (m->graph) cudaGraphDestroy(m->graph);
+        if (m->cap_stream) cudaStreamDestroy(m->cap_stream);
+        if (m->d_mem) cudaFree(m->d_mem);
+    }
+    for (zlfft_plan p : m->plans) release(p);
+    delete m;
+}
+
+int mixed_validate(const zlfft_desc& d, size_t i) {
+    if (d.kind != ZLFFT_C2C && d.kind != ZLFFT_R2C)
+        return fail(ZLFFT_ERR_INVALID_ARG, "descriptor %zu: invalid kind %d", i, d.kind);
+    if (d.precision != ZLFFT_F32 && d.precision != ZLFFT_F64)
+        return fail(ZLFFT_ERR_INVALID_ARG, "descriptor %zu: invalid precision %d", i, d.precision);
+    const int lo = d.kind == ZLFFT_C2C ? 0 : 1;
+    const int hi = zlfft::kPassMaxP + (d.kind == ZLFFT_C2C ? 0 : 1);
+    if (d.order < lo || d.order > hi)
+        return fail(ZLFFT_ERR_UNSUPPORTED, "descriptor %zu: order %d outside %d..%d", i, d.order, lo, hi);
+    if (d.op < ZLFFT_FORWARD || d.op > ZLFFT_FORWARD_SQR_MAG)
+        return fail(ZLFFT_ERR_INVALID_ARG, "descriptor %zu: invalid op %d", i, d.op);
+    if (d.op == ZLFFT_FORWARD_SQR_MAG && d.kind != ZLFFT_R2C)
+        return fail(ZLFFT_ERR_INVALID_ARG, "descriptor %zu: forward_sqr_mag is an RFFT operation", i);
+    if (!d.in || !d.out) return fail(ZLFFT_ERR_INVALID_ARG, "descriptor %zu: null buffer pointer", i);
+    const size_t es = d.precision == ZLFFT_F32 ? 4 : 8;
+    // complex values and real inputs are accessed as pairs; the sqr_mag output as reals
+    if (!aligned(d.in, 2 * es) || !aligned(d.out, d.op == ZLFFT_FORWARD_SQR_MAG ? es : 2 * es))
+        return fail(ZLFFT_ERR_ALIGNMENT, "descriptor %zu: buffers must be %zu-byte aligned", i, 2 * es);
+    return ZLFFT_OK;
+}
+
+// Cost of one persistent tile of complex order P (points x stages): orders
+// 4 and up hold 128 * 16 points per tile, so the cost grows with P.
+long long mixed_tile_cost(int P) { return (long long)zlfft::mixed_tpc(P) * (1LL << P) * (P > 0 ? P : 1); }
+
+zlfft::TileArgs mixed_args(const zlfft_mixed_s* m, const MixedGroupHost& g) {
+    zlfft::TileArgs a{};
+    a.batch = (long long)g.count;
+    a.tw = g.plan->d_tw;
+    a.tws = g.plan->d_tws;
+    a.rw = g.plan->d_rw;
+    a.err = g.plan->d_err;
+    a.tma = 0;
+    a.gin0 = m->d_gin + g.first;
+    a.gout0 = m->d_gout + g.first;
+    return a;
+}
+
+bool mixed_in_persistent(const MixedGroupHost& g) { return g.P >= zlfft::kMixedMinP && g.P <= zlfft::kMixedMaxP; }
+
+// One group as its own batched launch(es) on `st`.
+int mixed_run_group(zlfft_mixed_s* m, const MixedGroupHost& g, cudaStream_t st) {
+    zlfft::LaunchCtx ctx{m->num_sms, &m->launches};
+    const zlfft::TileArgs a = mixed_args(m, g);
+    if (g.P > zlfft::kTileMaxP) return exec_multipass(g.plan, g.dop, ZLFFT_AOS, ZLFFT_AOS, a, st, ctx);
+    const zlfft::GatherTable& t = g.prec == ZLFFT_F32 ? tables().g32 : tables().g64;
+    zlfft::TileLaunchFn fn = t.fn[g.P][g.dop];
+    if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no gathered kernel for order %d", g.P);
+    cudaError_t e = fn(a, st, ctx);
+    if (e != cudaSuccess) return cuda_fail(e, "gathered tile launch");
+    return ZLFFT_OK;
+}
+
+int mixed_run(zlfft_mixed_s* m, int schedule, cudaStream_t st) {
+    const bool persistent = schedule != ZLFFT_SCHED_PER_ORDER;
+    for (const MixedGroupHost& g : m->groups) {
+        if (persistent && mixed_in_persistent(g)) continue;
+        int rc = mixed_run_group(m, g, st);
+        if (rc) return rc;
+    }
+    if (!persistent) return ZLFFT_OK;
+    for (int pr = 0; pr < 2; ++pr) {
+        if (!m->n_items[pr]) continue;
+        ZL_CUDA(cudaMemsetAsync(m->d_counter + pr, 0, sizeof(int), st));
+        cudaError_t e = pr == 0 ? zlfft::launch_mixed_f32(m->d_mgroups[0], m->d_items[0], m->n_items[0],
+                                                          m->d_counter, st, m->num_sms)
+                                : zlfft::launch_mixed_f64(m->d_mgroups[1], m->d_items[1], m->n_items[1],
+                                                          m->d_counter + 1, st, m->num_sms);
+        if (e != cudaSuccess) return cuda_fail(e, "persistent mixed launch");
+        ++m->launches;
+    }
+    return ZLFFT_OK;
+}
+
+int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int device) {
+    if (!out) return fail(ZLFFT_ERR_INVALID_ARG, "mixed pointer is null");
+    *out = nullptr;
+    if (n && !descs) return fail(ZLFFT_ERR_INVALID_ARG, "null descriptor array");
+    if (n > (size_t)1 << 30) return fail(ZLFFT_ERR_INVALID_ARG, "too many descriptors");
+    for (size_t i = 0; i < n; ++i) {
+        int rc = mixed_validate(descs[i], i);
+        if (rc) return rc;
+    }
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return fail(ZLFFT_ERR_CUDA, "no CUDA device");
+    auto* m = new zlfft_mixed_s();
+    m->device = device;
+    DeviceGuard dg(device);
+    if (cudaDeviceGetAttribute(&m->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        mixed_release(m);
+        return fail(ZLFFT_ERR_CUDA, "cudaDeviceGetAttribute failed");
+    }
+    auto dop_of = [](const zlfft_desc& d) {
+        if (d.kind == ZLFFT_C2C) return d.op == ZLFFT_FORWARD ? (int)zlfft::kC2CFwd : (int)zlfft::kC2CBwd;
+        if (d.op == ZLFFT_FORWARD) return (int)zlfft::kR2CFwd;
+        if (d.op == ZLFFT_FORWARD_SQR_MAG) return (int)zlfft::kR2CSqrMag;
+        return (int)zlfft::kC2RBwd;
+    };
+    auto cplx_order = [](const zlfft_desc& d) { return d.kind == ZLFFT_C2C ? d.order : d.order - 1; };
+    // sort: complex order descending, then precision, kind, order, op (stable for the data order)
+    std::vector<size_t> idx(n);
+    for (size_t i = 0; i < n; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
+        const zlfft_desc &a = descs[x], &b = descs[y];
+        return std::make_tuple(-cplx_order(a), a.precision, a.kind, a.order, dop_of(a)) <
+               std::make_tuple(-cplx_order(b), b.precision, b.kind, b.order, dop_of(b));
+    });
+    std::map<std::tuple<int, int, int>, zlfft_plan> plan_of;  // (precision, kind, order)
+    std::vector<const void*> h_gin(n);
+    std::vector<void*> h_gout(n);
+    for (size_t j = 0; j < n; ++j) {
+        const zlfft_desc& d = descs[idx[j]];
+        h_gin[j] = d.in;
+        h_gout[j] = d.out;
+        const int dop = dop_of(d);
+        MixedGroupHost* g = m->groups.empty() ? nullptr : &m->groups.back();
+        if (!g || g->prec != d.precision || g->plan->kind != d.kind || g->plan->order != d.order || g->dop != dop) {
+            auto key = std::make_tuple(d.precision, d.kind, d.order);
+            auto it = plan_of.find(key);
+            if (it == plan_of.end()) {
+                zlfft_plan p = nullptr;
+                int rc = zlfft_plan_create(&p, d.kind, d.precision, (size_t)d.order, ZLFFT_MODE_PLAIN, device);
+                if (rc) {
+                    mixed_release(m);
+                    return rc;
+                }
+                m->plans.push_back(p);
+                if (p->cfft_order > zlfft::kTileMaxP && (rc = ensure_scratch(p)) != ZLFFT_OK) {
+                    mixed_release(m);
+                    return rc;
+                }
+                it = plan_of.emplace(key, p).first;
+            }
+            m->groups.push_back(MixedGroupHost{it->second, d.precision, dop, cplx_order(d), j, 0});
+            g = &m->groups.back();
+        }
+        ++g->count;
+    }
+    // device block: gather arrays, then per precision the group records and work lists
+    std::vector<zlfft::MixedGroup> mg[2];
+    std::vector<zlfft::MixedItem> items[2];
+    std::vector<long long> cost[2];
+    const size_t gin_off = 0, gout_off = n * sizeof(void*);
+    size_t off = 2 * n * sizeof(void*);
+    auto align_up = [](size_t v) { return (v + 255) & ~size_t{255}; };
+    for (const MixedGroupHost& g : m->groups) {
+        if (!mixed_in_persistent(g)) continue;
+        const int pr = g.prec == ZLFFT_F32 ? 0 : 1;
+        const int tpc = zlfft::mixed_tpc(g.P);
+        const long long tiles = ((long long)g.count + tpc - 1) / tpc;
+        for (long long t = 0; t < tiles; ++t) {
+            items[pr].push_back(zlfft::MixedItem{(int)mg[pr].size(), (int)t});
+            cost[pr].push_back(mixed_tile_cost(g.P));
+        }
+        mg[pr].push_back(zlfft::MixedGroup{zlfft::TileArgs{}, zlfft::mixed_code(g.dop, g.P)});
+    }
+    for (int pr = 0; pr < 2; ++pr) {
+        // longest tiles first (groups are already in descending order; keep it stable)
+        std::vector<size_t> o(items[pr].size());
+        for (size_t i = 0; i < o.size(); ++i) o[i] = i;
+        std::stable_sort(o.begin(), o.end(), [&](size_t x, size_t y) { return cost[pr][x] > cost[pr][y]; });
+        std::vector<zlfft::MixedItem> sorted(o.size());
+        for (size_t i = 0; i < o.size(); ++i) sorted[i] = items[pr][o[i]];
+        items[pr].swap(sorted);
+        if (items[pr].size() > (size_t)INT32_MAX) {
+            mixed_release(m);
+            return fail(ZLFFT_ERR_INVALID_ARG, "too many tiles");
+        }
+        m->n_items[pr] = (int)items[pr].size();
+    }
+    size_t grp_off[2], item_off[2];
+    for (int pr = 0; pr < 2; ++pr) {
+        off = align_up(off);
+        grp_off[pr] = off;
+        off += mg[pr].size() * sizeof(zlfft::MixedGroup);
+        off = align_up(off);
+        item_off[pr] = off;
+        off += items[pr].size() * sizeof(zlfft::MixedItem);
+    }
+    off = align_up(off);
+    const size_t counter_off = off;
+    off += 2 * sizeof(int);
+    if (cudaMalloc(&m->d_mem, off) != cudaSuccess) {
+        cudaGetLastError();
+        mixed_release(m);
+        return fail(ZLFFT_ERR_ALLOC, "mixed batch allocation of %zu bytes failed", off);
+    }
+    char* base = static_cast<char*>(m->d_mem);
+    m->d_gin = reinterpret_cast<const void**>(base + gin_off);
+    m->d_gout = reinterpret_cast<void**>(base + gout_off);
+    m->d_counter = reinterpret_cast<int*>(base + counter_off);
+    // group records now that the gather arrays have device addresses
+    {
+        size_t k[2] = {0, 0};
+        for (const MixedGroupHost& g : m->groups) {
+            if (!mixed_in_persistent(g)) continue;
+            const int pr = g.prec == ZLFFT_F32 ? 0 : 1;
+            mg[pr][k[pr]++].a = mixed_args(m, g);
+        }
+    }
+    cudaError_t e = cudaSuccess;
+    if (n) {
+        e = cudaMemcpy(base + gin_off, h_gin.data(), n * sizeof(void*), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(base + gout_off, h_gout.data(), n * sizeof(void*), cudaMemcpyHostToDevice);
+    }
+    for (int pr = 0; pr < 2 && e == cudaSuccess; ++pr) {
+        m->d_mgroups[pr] = reinterpret_cast<zlfft::MixedGroup*>(base + grp_off[pr]);
+        m->d_items[pr] = reinterpret_cast<zlfft::MixedItem*>(base + item_off[pr]);
+        if (!mg[pr].empty())
+            e = cudaMemcpy(m->d_mgroups[pr], mg[pr].data(), mg[pr].size() * sizeof(zlfft::MixedGroup),
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !items[pr].empty())
+            e = cudaMemcpy(m->d_items[pr], items[pr].data(), items[pr].size() * sizeof(zlfft::MixedItem),
+                           cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemset(m->d_counter, 0, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&m->cap_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        mixed_release(m);
+        return cuda_fail(e, "mixed batch set-up");
+    }
+    *out = m;
+    return ZLFFT_OK;
+}
+
+// The persistent schedule recorded once into a graph (on the batch's own
+// stream, relaxed capture mode), replayed on the caller's stream.
+int mixed_graph(zlfft_mixed_s* m, cudaStream_t st) {
+    if (!m->graph_exec) {
+        const size_t before = m->launches;
+        ZL_CUDA(cudaStreamBeginCapture(m->cap_stream, cudaStreamCaptureModeRelaxed));
+        int rc = mixed_run(m, ZLFFT_SCHED_PERSISTENT, m->cap_stream);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(m->cap_stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        m->graph = graph;
+        ZL_CUDA(cudaGraphInstantiate(&m->graph_exec, m->graph, 0));
+        m->graph_launches = m->launches - before;
+        m->launches = before;
+    }
+    ZL_CUDA(cudaGraphLaunch(m->graph_exec, st));
+    m->launches += m->graph_launches;
+    return ZLFFT_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -963,6 +1288,61 @@ int zlfft_selftest_bounded_wait(int device, int* status) {
     cudaFree(d);
     if (e != cudaSuccess) return cuda_fail(e, "selftest");
     return ZLFFT_OK;
+}
+
+int zlfft_mixed_create(zlfft_mixed* mixed, const zlfft_desc* descs, size_t n, int device) {
+    return mixed_create_impl(mixed, descs, n, device);
+}
+
+int zlfft_mixed_exec(zlfft_mixed mixed, int schedule, void* stream) {
+    if (!mixed) return fail(ZLFFT_ERR_INVALID_ARG, "null mixed batch");
+    if (schedule < ZLFFT_SCHED_PER_ORDER || schedule > ZLFFT_SCHED_GRAPH)
+        return fail(ZLFFT_ERR_INVALID_ARG, "invalid schedule %d", schedule);
+    std::lock_guard<std::mutex> lock(mixed->mu);
+    DeviceGuard g(mixed->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (schedule == ZLFFT_SCHED_GRAPH) return mixed_graph(mixed, st);
+    return mixed_run(mixed, schedule, st);
+}
+
+int zlfft_mixed_take_launch_count(zlfft_mixed mixed, size_t* launches) {
+    if (!mixed || !launches) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lock(mixed->mu);
+    *launches = mixed->launches;
+    mixed->launches = 0;
+    return ZLFFT_OK;
+}
+
+int zlfft_mixed_device_status(zlfft_mixed mixed, int* status) {
+    if (!mixed || !status) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    int any = 0;
+    for (zlfft_plan p : mixed->plans) {
+        int s = 0;
+        int rc = zlfft_plan_device_status(p, &s);
+        if (rc && rc != ZLFFT_ERR_DEVICE_TIMEOUT) return rc;
+        any |= s;
+    }
+    *status = any;
+    return any ? ZLFFT_ERR_DEVICE_TIMEOUT : ZLFFT_OK;
+}
+
+int zlfft_mixed_destroy(zlfft_mixed mixed) {
+    mixed_release(mixed);
+    return ZLFFT_OK;
+}
+
+int zlfft_exec_mixed_device(const zlfft_desc* descs, size_t n, void* stream) {
+    zlfft_mixed m = nullptr;
+    int rc = mixed_create_impl(&m, descs, n, -1);
+    if (rc) return rc;
+    {
+        DeviceGuard g(m->device);
+        rc = mixed_run(m, ZLFFT_SCHED_PERSISTENT, static_cast<cudaStream_t>(stream));
+        const cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+        if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamSynchronize");
+    }
+    mixed_release(m);
+    return rc;
 }
 
 const char* zlfft_last_error(void) { return g_last_error.c_str(); }

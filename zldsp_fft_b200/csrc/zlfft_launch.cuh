@@ -54,6 +54,43 @@ cudaError_t launch_tile(const TileArgs& a, cudaStream_t stream, const LaunchCtx&
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ gathered tile launches
+// Tile kernels reading/writing per-transform pointers (mixed batches), for
+// the AoS <-> AoS operations: [order][op].
+struct GatherTable {
+    TileLaunchFn fn[kTileMaxP + 1][5];
+};
+
+template <typename F, int P, int OP>
+cudaError_t launch_tile_gather(const TileArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
+    using Cfg = TileCfg<F, P, OP>;
+    auto kern = tile_kernel<F, P, OP, kAoS, kAoS, true>;
+    static const int blocks_per_sm = [kern]() {
+        if (Cfg::SMEM > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, Cfg::THREADS, Cfg::SMEM) != cudaSuccess || b < 1)
+            b = 1;
+        return b;
+    }();
+    if (a.batch <= 0) return cudaSuccess;
+    const long long tiles = (a.batch + Cfg::TPC - 1) / Cfg::TPC;
+    const long long cap = (long long)ctx.num_sms * blocks_per_sm;
+    const unsigned grid = (unsigned)(tiles < cap ? tiles : cap);
+    kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(a);
+    if (ctx.launches) ++*ctx.launches;
+    return cudaGetLastError();
+}
+
+template <typename F, int... Ps>
+void fill_gather_orders(GatherTable& t, std::integer_sequence<int, Ps...>) {
+    ((t.fn[Ps][kC2CFwd] = launch_tile_gather<F, Ps, kC2CFwd>, t.fn[Ps][kC2CBwd] = launch_tile_gather<F, Ps, kC2CBwd>,
+      t.fn[Ps][kR2CFwd] = launch_tile_gather<F, Ps, kR2CFwd>, t.fn[Ps][kR2CSqrMag] = launch_tile_gather<F, Ps, kR2CSqrMag>,
+      t.fn[Ps][kC2RBwd] = launch_tile_gather<F, Ps, kC2RBwd>),
+     ...);
+}
+void fill_gather_f32(GatherTable& t);
+void fill_gather_f64(GatherTable& t);
+
 // ------------------------------------------------------------------ multi-pass
 constexpr int kPassMinP = 14;
 constexpr int kPassMaxP = 24;
@@ -125,7 +162,7 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
         const char* e = getenv("ZLFFT_PASS_TMA");
         return !(e && e[0] == '0');
     }();
-    a.tma = (tma_enabled && a.tma && encode_pass_maps<F, P, PI, IL2>(a, maps)) ? 1 : 0;
+    a.tma = (tma_enabled && a.tma && !(Cfg::FIRST && a.gin0) && encode_pass_maps<F, P, PI, IL2>(a, maps)) ? 1 : 0;
     static const int blocks_per_sm = [kern]() {
         if (Cfg::SMEM > 48 * 1024)
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);

@@ -106,6 +106,12 @@ struct PassArgs {
     const void* tws;       // per-stage twiddle tables (stage_l0 layout)
     int* err;              // device error word (kDevErrWaitTimeout on a timed-out wait)
     int tma;               // the tensor maps describe the input (else direct loads)
+    // Gathered transforms (mixed batches): the first pass reads transform t
+    // at gin0[t] (gin1[t]) and the last pass writes it at gout0[t] (gout1[t]).
+    const void* const* gin0;
+    const void* const* gin1;
+    void* const* gout0;
+    void* const* gout1;
 };
 
 // Tensor maps of a pass input, encoded on the host (zlfft_launch.cuh): a 3-D
@@ -215,7 +221,9 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                             __syncthreads();           // staging fully read: refill it with the next item
                             issue(item + gridDim.x);
                         } else {
-                            const CxIn<F, IL2> in(a.in0, a.in1, tr * a.in_stride);
+                            const bool g = Cfg::FIRST && a.gin0 != nullptr;
+                            const CxIn<F, IL2> in(g ? a.gin0[tr] : a.in0, g ? (a.gin1 ? a.gin1[tr] : nullptr) : a.in1,
+                                                  g ? 0 : tr * a.in_stride);
 #pragma unroll
                             for (int i = 0; i < NB; ++i) {
                                 const int b = tb + i * T;
@@ -266,7 +274,9 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                             for (int s = 0; s < G.R; ++s) sm[(b + group_mu(G, s) * ELL) * ROW + u] = v[i * G.R + s];
                         }
                         __syncthreads();
-                        const CxOut<F, OL2> out(a.out0, a.out1, tr * a.out_stride + (long long)(U - u) * R);
+                        const bool g = Cfg::LAST && a.gout0 != nullptr;
+                        const CxOut<F, OL2> out(g ? a.gout0[tr] : a.out0, g ? (a.gout1 ? a.gout1[tr] : nullptr) : a.out1,
+                                                (g ? 0 : tr * a.out_stride) + (long long)(U - u) * R);
 #pragma unroll 4
                         for (int e = (int)threadIdx.x; e < UPC * R; e += Cfg::THREADS) {
                             const int uu = e / R, pos = e % R;
@@ -275,7 +285,9 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                         }
                         __syncthreads();
                     } else {
-                        const CxOut<F, OL2> out(a.out0, a.out1, tr * a.out_stride + (long long)J * L_OUT + ku);
+                        const bool g = Cfg::LAST && a.gout0 != nullptr;
+                        const CxOut<F, OL2> out(g ? a.gout0[tr] : a.out0, g ? (a.gout1 ? a.gout1[tr] : nullptr) : a.out1,
+                                                (g ? 0 : tr * a.out_stride) + (long long)J * L_OUT + ku);
 #pragma unroll
                         for (int i = 0; i < NB; ++i) {
                             const int b = tb + i * T;
@@ -302,7 +314,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
 // One thread per bin pair (k, M - k), k = 0 .. M/2 (k = 0 is DC/Nyquist).
 template <typename F, int OP, int LAYOUT>
 __global__ void rfft_split_kernel(const Cx<F>* z, void* out0, void* out1, const Cx<F>* rw, int M, long long batch,
-                                  long long z_stride, long long out_stride) {
+                                  long long z_stride, long long out_stride, void* const* gout0, void* const* gout1) {
     using C = Cx<F>;
     const long long pairs = (long long)(M / 2 + 1);
     const long long total = pairs * batch;
@@ -311,8 +323,11 @@ __global__ void rfft_split_kernel(const Cx<F>* z, void* out0, void* out1, const 
         const int k = (int)(i % pairs);
         const C* zt = z + tr * z_stride;
         constexpr int OL2 = (OP == kR2CSqrMag) ? (int)kAoS : LAYOUT;
-        const CxOut<F, OL2> out(out0, out1, tr * out_stride);
-        F* osq = static_cast<F*>(out0) + tr * out_stride;
+        void* o0 = gout0 ? gout0[tr] : out0;
+        void* o1 = gout0 ? (gout1 ? gout1[tr] : nullptr) : out1;
+        const long long ob = gout0 ? 0 : tr * out_stride;
+        const CxOut<F, OL2> out(o0, o1, ob);
+        F* osq = static_cast<F*>(o0) + ob;
         if (k == 0) {
             const C z0 = zt[0];
             const F dc = z0.x + z0.y, ny = z0.x - z0.y;
@@ -339,14 +354,16 @@ __global__ void rfft_split_kernel(const Cx<F>* z, void* out0, void* out1, const 
 
 template <typename F, int LAYOUT>
 __global__ void rfft_pre_kernel(const void* in0, const void* in1, Cx<F>* z, const Cx<F>* rw, int M, long long batch,
-                                long long in_stride, long long z_stride) {
+                                long long in_stride, long long z_stride, const void* const* gin0,
+                                const void* const* gin1) {
     using C = Cx<F>;
     const long long pairs = (long long)(M / 2 + 1);
     const long long total = pairs * batch;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
         const long long tr = i / pairs;
         const int k = (int)(i % pairs);
-        const CxIn<F, LAYOUT> in(in0, in1, tr * in_stride);
+        const CxIn<F, LAYOUT> in(gin0 ? gin0[tr] : in0, gin0 ? (gin1 ? gin1[tr] : nullptr) : in1,
+                                 gin0 ? 0 : tr * in_stride);
         C* zt = z + tr * z_stride;
         if (k == 0) {
             const C x0 = in[0], xm = in[M];

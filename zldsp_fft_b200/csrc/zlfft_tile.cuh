@@ -120,15 +120,22 @@ struct TileArgs {
     const void* rw;        // RFFT split twiddles (0.5*cos, 0.5*sin + 0.5) pairs, k = 0..N/2
     int* err;              // device error word (kDevErrWaitTimeout on a timed-out wait)
     int tma;               // inputs qualify for bulk copies (16-byte aligned bases and strides)
+    // Gathered transforms (mixed batches): when gin0 is set, transform t reads
+    // from gin0[t] (and gin1[t] for split SoA) and writes to gout0[t] (gout1[t]);
+    // the strides are then unused.
+    const void* const* gin0;
+    const void* const* gin1;
+    void* const* gout0;
+    void* const* gout1;
 };
 
-template <typename F, int P, int OP = kC2CFwd>
+template <typename F, int P, int OP = kC2CFwd, int BLOCK = 128>
 struct TileCfg {
     using C = Cx<F>;
     static constexpr int N = 1 << P;
     static constexpr int E = tile_elems(P);
     static constexpr int T = N / E;  // threads per transform
-    static constexpr int TPC = T >= 128 ? 1 : 128 / T;
+    static constexpr int TPC = T >= BLOCK ? 1 : BLOCK / T;
     static constexpr int THREADS = T * TPC;
     static constexpr size_t XBYTES = (size_t)TPC * N * sizeof(C);  // exchange buffer
     // Staging buffer for the next tile's input, filled by TMA bulk copies
@@ -360,86 +367,70 @@ __device__ __forceinline__ SplitOut<F> rfft_split(C z1, C z2, F c, F s) {
     return o;
 }
 
-// ---------------------------------------------------------------- the kernel
-template <typename F, int P, int OP, int IL, int OL>
-__global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>::MINB) tile_kernel(const TileArgs a) {
-    using Cfg = TileCfg<F, P, OP>;
+// ---------------------------------------------------------------- the tile worker
+// Per-thread state of one CTA working on tiles of TPC transforms of order P,
+// and the processing of one tile. tile_kernel drives it over a contiguous
+// batch with TMA prefetch; mixed_kernel (zlfft_mixed.cuh) drives it over a
+// queue of tiles of many orders.
+template <typename F, int P, int OP, int IL, int OL, int BLOCK = 128, bool GATHER = false>
+struct TileWorker {
+    using Cfg = TileCfg<F, P, OP, BLOCK>;
     using C = Cx<F>;
-    constexpr int N = Cfg::N, E = Cfg::E, T = Cfg::T, TPC = Cfg::TPC, NG = Cfg::NG;
-    constexpr bool kFwd = (OP == kC2CFwd || OP == kR2CFwd || OP == kR2CSqrMag);
-    constexpr bool kR2C = (OP == kR2CFwd || OP == kR2CSqrMag);
-    constexpr Grp GL = tile_group(P, NG > 0 ? NG - 1 : 0);
+    static constexpr int N = Cfg::N, E = Cfg::E, T = Cfg::T, TPC = Cfg::TPC, NG = Cfg::NG;
+    static constexpr bool kFwd = (OP == kC2CFwd || OP == kR2CFwd || OP == kR2CSqrMag);
+    static constexpr bool kR2C = (OP == kR2CFwd || OP == kR2CSqrMag);
+    static constexpr Grp GL = tile_group(P, NG > 0 ? NG - 1 : 0);
     // last group: one butterfly per thread, twiddles held in registers (FP32;
     // FP64 twiddles would take twice the registers and are read from L1)
-    constexpr bool kLastReg = NG >= 2 && GL.R == E && !GL.first && sizeof(F) == 4;
-    constexpr bool kShufPost = kR2C && NG >= 2 && GL.R == E && !GL.first && GL.R == 16 && T >= 2;
-    constexpr int kLastTw = group_tw_count<P, GL.R, GL.L, GL.first>();
+    static constexpr bool kLastReg = NG >= 2 && GL.R == E && !GL.first && sizeof(F) == 4;
+    static constexpr bool kShufPost = kR2C && NG >= 2 && GL.R == E && !GL.first && GL.R == 16 && T >= 2;
+    static constexpr int kLastTw = group_tw_count<P, GL.R, GL.L, GL.first>();
+    static constexpr int H = (T < 32 ? T : 32) / 2;  // partner-lane distance of the shuffle split
+    static constexpr bool kSoAIn = (IL == kSoA) && !kR2C;
 
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* sm = reinterpret_cast<C*>(smem_raw);
-    const int lt = (int)threadIdx.x % T;
-    const int slot = (int)threadIdx.x / T;
-    const uint32_t sbase = (uint32_t)slot * N;
-    auto sidx = [&](int pos) -> uint32_t { return swz<C>(sbase + (uint32_t)pos); };
-    const C* tw = static_cast<const C*>(a.tw);
-    const C* tws = static_cast<const C*>(a.tws);
-
-    const int b_last = last_butterfly<kShufPost, T>(lt, GL.L);
-    constexpr int H = (T < 32 ? T : 32) / 2;  // partner-lane distance of the shuffle split
+    C* sm;
+    int lt, slot;
+    uint32_t sbase;
+    const C* tw;
+    const C* tws;
+    int b_last;
     C wl[kLastTw > 0 ? kLastTw : 1];
-    if constexpr (kLastReg) group_load_tw<P, GL.R, GL.L, GL.first>(tw, (uint32_t)(b_last % GL.L), wl);
 
-    // ---- TMA staging of each tile's input (one tile ahead)
-    constexpr bool kSoAIn = (IL == kSoA) && !kR2C;
-    C* stage = sm + (size_t)TPC * N;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::XBYTES * 2);
-    const bool use_tma = Cfg::kTMA && a.tma;
-    auto issue = [&](long long t) {  // warp 0 issues the copies of tile t
-        if (!use_tma || threadIdx.x >= 32 || t * TPC >= a.batch) return;
-        const long long left = a.batch - t * TPC;
-        const int nvalid = (int)(left < TPC ? left : TPC);
-        constexpr uint32_t kSlot = (uint32_t)(N * sizeof(C));
-        if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, kSlot * (uint32_t)nvalid);
-        __syncwarp();
-        for (int q = (int)threadIdx.x; q < nvalid; q += 32) {
-            const long long base = (t * TPC + q) * a.in_stride;
-            if constexpr (kSoAIn) {
-                F* dst = reinterpret_cast<F*>(stage + (size_t)q * N);
-                bulk_g2s(dst, static_cast<const F*>(a.in0) + base, kSlot / 2, bar);
-                bulk_g2s(dst + N, static_cast<const F*>(a.in1) + base, kSlot / 2, bar);
-            } else {
-                bulk_g2s(stage + (size_t)q * N, static_cast<const C*>(a.in0) + base, kSlot, bar);
-            }
-        }
-    };
-    if constexpr (Cfg::kTMA) {
-        if (use_tma) {
-            if (threadIdx.x == 0) {
-                mbar_init(bar, 1);
-                fence_mbar_init();
-            }
-            __syncthreads();
-            issue(blockIdx.x);
-        }
+    __device__ __forceinline__ TileWorker(const TileArgs& a, unsigned char* smem_raw) {
+        sm = reinterpret_cast<C*>(smem_raw);
+        lt = (int)threadIdx.x % T;
+        slot = (int)threadIdx.x / T;
+        sbase = (uint32_t)slot * N;
+        tw = static_cast<const C*>(a.tw);
+        tws = static_cast<const C*>(a.tws);
+        b_last = last_butterfly<kShufPost, T>(lt, GL.L);
+        if constexpr (kLastReg) group_load_tw<P, GL.R, GL.L, GL.first>(tw, (uint32_t)(b_last % GL.L), wl);
     }
-    uint32_t phase = 0;
 
-    for (long long tile = blockIdx.x; tile * TPC < a.batch; tile += gridDim.x) {
-        if constexpr (Cfg::kTMA) {
-            if (use_tma) {
-                const bool ok = mbar_wait(bar, phase);
-                if (__syncthreads_or(!ok)) {  // bounded wait ran out: report and leave
-                    if (threadIdx.x == 0) atomicOr(a.err, kDevErrWaitTimeout);
-                    mbar_wait(bar, phase);  // give copies in flight a bounded chance to land
-                    return;
-                }
-                phase ^= 1u;
-            }
-        }
+    __device__ __forceinline__ uint32_t sidx(int pos) const { return swz<C>(sbase + (uint32_t)pos); }
+
+    // Process tile `tile`. With a staging buffer, group 0 reads this tile's
+    // input from it (placed there by TMA) and calls refill() once done.
+    template <class Refill>
+    __device__ __forceinline__ void run(const TileArgs& a, long long tile, const C* stage, Refill&& refill) {
+        const bool use_tma = stage != nullptr;
         const long long tr = tile * TPC + slot;
         const bool valid = tr < a.batch;
-        const long long ibase = valid ? tr * a.in_stride : 0;
-        const long long obase = valid ? tr * a.out_stride : 0;
+        // this slot's transform: contiguous (base + stride) or gathered pointers
+        const void* ib0 = a.in0;
+        const void* ib1 = a.in1;
+        void* ob0 = a.out0;
+        void* ob1 = a.out1;
+        long long ibase = valid ? tr * a.in_stride : 0;
+        long long obase = valid ? tr * a.out_stride : 0;
+        if constexpr (GATHER) {
+            const long long g = valid ? tr : 0;
+            ib0 = a.gin0[g];
+            ib1 = a.gin1 ? a.gin1[g] : nullptr;
+            ob0 = a.gout0[g];
+            ob1 = a.gout1 ? a.gout1[g] : nullptr;
+            ibase = obase = 0;
+        }
         C v[E];
 
         // ------------------------------------------------ input
@@ -447,7 +438,7 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
             // Backward RFFT pre-step into shared memory (execute.hpp:399-451).
             if (valid) {
                 const C* rw = static_cast<const C*>(a.rw);
-                const CxIn<F, IL> in(a.in0, a.in1, ibase);
+                const CxIn<F, IL> in(ib0, ib1, ibase);
                 for (int k = 1 + lt; k <= N / 2; k += T) {
                     const C x1 = in[k];
                     const C x2 = in[N - k];
@@ -470,14 +461,14 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
 
         // ------------------------------------------------ stage groups
         constexpr int OL2 = (OP == kC2RBwd || OP == kR2CSqrMag) ? (int)kAoS : OL;
-        const CxOut<F, OL2> out(a.out0, a.out1, obase);
+        const CxOut<F, OL2> out(ob0, ob1, obase);
         if constexpr (NG == 0) {
             C x;
             if constexpr (OP == kC2RBwd) {
                 x = cswap(sm[sidx(0)]);
             } else {
                 constexpr int IL2 = kR2C ? (int)kAoS : IL;
-                const CxIn<F, IL2> in(a.in0, a.in1, ibase);
+                const CxIn<F, IL2> in(ib0, ib1, ibase);
                 x = valid ? in[0] : cx<C>((F)0, (F)0);
                 if constexpr (!kFwd) x = cswap(x);
             }
@@ -509,12 +500,10 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
                                         v[u * G.R + rho] = kFwd ? x : cswap(x);
                                     }
                                 }
-                                fence_proxy_async_smem();  // reads of the staging buffer before its TMA refill
-                                __syncthreads();           // staging fully read: refill it with the next tile
-                                issue(tile + gridDim.x);
+                                refill();
                             } else {
                                 constexpr int IL2 = kR2C ? (int)kAoS : IL;
-                                const CxIn<F, IL2> in(a.in0, a.in1, ibase);
+                                const CxIn<F, IL2> in(ib0, ib1, ibase);
 #pragma unroll
                                 for (int u = 0; u < NB; ++u) {
                                     const int b = (kLast ? b_last : lt) + u * T;
@@ -582,7 +571,7 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
 #pragma unroll
                             for (int s = 0; s < 16; ++s) z[group_mu(G, s)] = v[s];
                             const C* rw = static_cast<const C*>(a.rw);
-                            [[maybe_unused]] F* osq = static_cast<F*>(a.out0) + obase;
+                            [[maybe_unused]] F* osq = static_cast<F*>(ob0) + obase;
 #pragma unroll
                             for (int m = 0; m < 8; ++m) {
                                 C p;
@@ -647,7 +636,7 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
             __syncthreads();
             if (valid) {
                 const C* rw = static_cast<const C*>(a.rw);
-                [[maybe_unused]] F* osq = static_cast<F*>(a.out0) + obase;
+                [[maybe_unused]] F* osq = static_cast<F*>(ob0) + obase;
                 for (int k = 1 + lt; k <= N / 2; k += T) {
                     const C w = rw[k];
                     const SplitOut<F> o = rfft_split<F>(sm[sidx(k)], sm[sidx(N - k)], w.x, w.y);
@@ -675,6 +664,71 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
         // The next tile's first shared-memory write is preceded by a barrier in
         // every path except the backward RFFT pre-step and the single-point case.
         if constexpr (OP == kC2RBwd || NG == 0) __syncthreads();
+    }
+};
+
+// ---------------------------------------------------------------- the kernel
+template <typename F, int P, int OP, int IL, int OL, bool GATHER = false>
+__global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>::MINB) tile_kernel(const TileArgs a) {
+    using W = TileWorker<F, P, OP, IL, OL, 128, GATHER>;
+    using Cfg = typename W::Cfg;
+    using C = Cx<F>;
+    constexpr int N = Cfg::N, TPC = Cfg::TPC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    W w(a, smem_raw);
+
+    // ---- TMA staging of each tile's input (one tile ahead)
+    constexpr bool kSoAIn = W::kSoAIn;
+    C* stage = reinterpret_cast<C*>(smem_raw) + (size_t)TPC * N;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::XBYTES * 2);
+    const bool use_tma = Cfg::kTMA && !GATHER && a.tma;
+    auto issue = [&](long long t) {  // warp 0 issues the copies of tile t
+        if (!use_tma || threadIdx.x >= 32 || t * TPC >= a.batch) return;
+        const long long left = a.batch - t * TPC;
+        const int nvalid = (int)(left < TPC ? left : TPC);
+        constexpr uint32_t kSlot = (uint32_t)(N * sizeof(C));
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, kSlot * (uint32_t)nvalid);
+        __syncwarp();
+        for (int q = (int)threadIdx.x; q < nvalid; q += 32) {
+            const long long base = (t * TPC + q) * a.in_stride;
+            if constexpr (kSoAIn) {
+                F* dst = reinterpret_cast<F*>(stage + (size_t)q * N);
+                bulk_g2s(dst, static_cast<const F*>(a.in0) + base, kSlot / 2, bar);
+                bulk_g2s(dst + N, static_cast<const F*>(a.in1) + base, kSlot / 2, bar);
+            } else {
+                bulk_g2s(stage + (size_t)q * N, static_cast<const C*>(a.in0) + base, kSlot, bar);
+            }
+        }
+    };
+    if constexpr (Cfg::kTMA) {
+        if (use_tma) {
+            if (threadIdx.x == 0) {
+                mbar_init(bar, 1);
+                fence_mbar_init();
+            }
+            __syncthreads();
+            issue(blockIdx.x);
+        }
+    }
+    uint32_t phase = 0;
+
+    for (long long tile = blockIdx.x; tile * TPC < a.batch; tile += gridDim.x) {
+        if constexpr (Cfg::kTMA) {
+            if (use_tma) {
+                const bool ok = mbar_wait(bar, phase);
+                if (__syncthreads_or(!ok)) {  // bounded wait ran out: report and leave
+                    if (threadIdx.x == 0) atomicOr(a.err, kDevErrWaitTimeout);
+                    mbar_wait(bar, phase);  // give copies in flight a bounded chance to land
+                    return;
+                }
+                phase ^= 1u;
+            }
+        }
+        w.run(a, tile, use_tma ? stage : nullptr, [&]() {
+            fence_proxy_async_smem();  // reads of the staging buffer before its TMA refill
+            __syncthreads();           // staging fully read: refill it with the next tile
+            issue(tile + gridDim.x);
+        });
     }
 }
 

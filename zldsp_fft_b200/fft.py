@@ -203,3 +203,52 @@ class RFFT:
     @property
     def plan(self) -> Plan:
         return self._plan
+
+
+class MixedBatch:
+    """Transforms of many orders and kinds in one call (zlfft_mixed_*).
+
+    ``descs`` is a sequence of ``(kind, order, op, in_ptr, out_ptr)`` tuples
+    (device pointers as ints, AoS buffers), all of precision ``dtype``, or of
+    ``(kind, order, op, in_ptr, out_ptr, precision)`` to mix precisions.
+    ``run(schedule)`` executes the whole batch on ``stream``; the schedules
+    are SCHED_PER_ORDER (one batched launch per order group),
+    SCHED_PERSISTENT (orders up to 2^11 complex in one persistent launch) and
+    SCHED_GRAPH (the persistent schedule replayed from a CUDA graph).
+    """
+
+    def __init__(self, descs, dtype=np.float32, device: int = -1):
+        self._lib = C.lib()
+        prec = _prec(dtype)
+        arr = (C.Desc * max(len(descs), 1))()
+        for i, d in enumerate(descs):
+            kind, order, op, ip, op_ptr = d[:5]
+            arr[i] = C.Desc(kind, d[5] if len(d) > 5 else prec, int(order), op, int(ip), int(op_ptr))
+        h = ctypes.c_void_p()
+        C.check(self._lib.zlfft_mixed_create(ctypes.byref(h), arr, len(descs), device))
+        self.handle = h
+        self.size = len(descs)
+
+    def run(self, schedule: int = C.SCHED_PERSISTENT, stream=0) -> None:
+        C.check(self._lib.zlfft_mixed_exec(self.handle, schedule, stream))
+
+    def take_launch_count(self) -> int:
+        v = ctypes.c_size_t()
+        C.check(self._lib.zlfft_mixed_take_launch_count(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def device_status(self) -> int:
+        v = ctypes.c_int()
+        self._lib.zlfft_mixed_device_status(self.handle, ctypes.byref(v))
+        return v.value
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            self._lib.zlfft_mixed_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
