@@ -508,7 +508,238 @@ class Mixed:
         return nbytes, dt
 
 
-WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G, "mixed": Mixed}
+class Cfft64:
+    """CFFT<double> order 16, batch 512, re, im ~ U[-1, 1) (seed 1005): one
+    step = forward then backward of the batch on the FP64 path (FP64
+    twiddles and butterflies). CFFT<float> at the same shape is timed beside
+    it, and a sample's error against numpy's FP64 FFT is reported."""
+    name = "cfft64"
+    desc = "CFFT<double> order 16 (N=65536) x 512, forward + backward, full FP64 path"
+    l2 = "each op reads 512 MiB and writes 512 MiB, > 4x L2 (no L2 flush needed)"
+    order, batch = 16, 512
+    dtype = "f64"
+
+    def __init__(self):
+        n = 1 << self.order
+        self.op_bytes = {"c2c_f64_fwd": 2 * 16 * n * self.batch, "c2c_f64_bwd": 2 * 16 * n * self.batch}
+        self.bytes_per_step = sum(self.op_bytes.values())
+        self.dominant = "c2c_f64_fwd"
+        self.host_in = None
+
+    def setup(self, device):
+        import torch
+        import zldsp_fft_b200 as Z
+        self.Z = Z
+        n = 1 << self.order
+        self.plan = Z.Plan(Z.C2C, self.order, np.float64, device=device)
+        g = torch.Generator(device=device)
+        g.manual_seed(1005)
+        self.A = (torch.rand((self.batch, n, 2), generator=g, device=device, dtype=torch.float64) * 2 - 1)
+        self.B = torch.empty_like(self.A)
+        self.C = torch.empty_like(self.A)
+        torch.cuda.synchronize(device)
+
+    def ops(self, step):
+        Z, p, b = self.Z, self.plan, self.batch
+        return [("c2c_f64_fwd", lambda st: p.exec_device(Z.FORWARD, Z.AOS, Z.AOS, self.A.data_ptr(), None,
+                                                         self.B.data_ptr(), None, b, stream=st)),
+                ("c2c_f64_bwd", lambda st: p.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, self.B.data_ptr(), None,
+                                                         self.C.data_ptr(), None, b, stream=st))]
+
+    def take_launches(self):
+        return self.plan.take_launch_count()
+
+    def compare(self, stream, reps):
+        """CFFT<float> at the same shape, and the FP64 error of a sample."""
+        import torch
+        Z = self.Z
+        n, b = 1 << self.order, self.batch
+        p32 = Z.Plan(Z.C2C, self.order, np.float32, device=self.A.device.index)
+        a32 = self.A.float()
+        b32 = torch.empty_like(a32)
+        c32 = torch.empty_like(a32)
+
+        def f32_step():
+            p32.exec_device(Z.FORWARD, Z.AOS, Z.AOS, a32.data_ptr(), None, b32.data_ptr(), None, b,
+                            stream=stream.cuda_stream)
+            p32.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, b32.data_ptr(), None, c32.data_ptr(), None, b,
+                            stream=stream.cuda_stream)
+        for _ in range(2):
+            f32_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            f32_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms32 = e0.elapsed_time(e1) / reps
+        f32_bytes = self.bytes_per_step // 2  # complex64 moves half the bytes
+        x = self.A[:8].cpu().numpy().view(np.complex128)[..., 0]
+        y64 = self.B[:8].cpu().numpy().view(np.complex128)[..., 0]
+        y32 = b32[:8].cpu().numpy().astype(np.float64).view(np.complex128)[..., 0]
+        ref = np.fft.fft(x, axis=-1)
+        nrm = np.linalg.norm(ref, axis=-1)
+        return {
+            "cfft_float_same_shape": {"gbs": round(f32_bytes / (ms32 / 1e3) / 1e9, 1), "ms_per_step": round(ms32, 4),
+                                      "transforms_per_s": round(2 * b / (ms32 / 1e3))},
+            "max_rel_l2_vs_numpy_fp64": {"f64": float((np.linalg.norm(y64 - ref, axis=-1) / nrm).max()),
+                                         "f32": float((np.linalg.norm(y32 - ref, axis=-1) / nrm).max())},
+            "tolerance": {"f64": 4 * 16 * 2.0 ** -53, "f32": 4 * 16 * 2.0 ** -24},
+        }
+
+    def cpu_sample_desc(self, frames):
+        return f"forward+backward of {frames} of the 512 transforms, median of 3"
+
+    def setup_e2e(self):
+        import torch
+        self.hA = self.A.cpu().pin_memory()
+        self.hB = torch.empty_like(self.hA).pin_memory()
+        self.e2e_h2d = 2 * self.hA.numel() * 8
+        self.e2e_d2h = 2 * self.hA.numel() * 8
+
+    def e2e_step(self):
+        Z, p, b = self.Z, self.plan, self.batch
+        p.exec_host(Z.FORWARD, Z.AOS, Z.AOS, self.hA.data_ptr(), None, self.hB.data_ptr(), None, b)
+        p.exec_host(Z.BACKWARD, Z.AOS, Z.AOS, self.hB.data_ptr(), None, self.hB.data_ptr(), None, b)
+
+    def cpu_run(self, frames, threads, kind):
+        from oracle import oracle as O
+        rng = np.random.default_rng(1005)
+        n = 1 << self.order
+        cnt = max(1, min(frames, self.batch))
+        x = rng.uniform(-1, 1, (cnt, n)) + 1j * rng.uniform(-1, 1, (cnt, n))
+        if kind == "reference":
+            plan = O.RefPlan("c2c", self.order, "f64", threads)
+            y, z = np.empty_like(x), np.empty_like(x)
+            t0 = time.perf_counter()
+            plan.cfft(x, True, out=y)
+            plan.cfft(y, False, out=z)
+            dt = time.perf_counter() - t0
+            plan.close()
+        else:
+            t0 = time.perf_counter()
+            O.cfft_port(O.cfft_port(x, True), False)
+            dt = time.perf_counter() - t0
+        return 2 * 2 * 16 * n * cnt, dt
+
+
+class Cfft10:
+    """CFFT<float> order 10 (N = 1024), one transform, AoS, re, im ~ U[-1, 1)
+    (seed 1001): one step = forward then backward of the single transform.
+    Latency-bound (16 KiB per direction): the line reports microseconds per
+    transform beside the GB/s; L2 is flushed (a 256 MiB write) between steps,
+    outside the timed ops."""
+    name = "cfft10"
+    desc = ("CFFT<float> order 10 (N=1024), single transform, forward then backward, AoS; each direction "
+            "replayed from a CUDA graph")
+    l2 = "L2 flushed between steps by a 256 MiB write, outside the timed ops"
+    order, batch = 10, 1
+    dtype = "f32"
+
+    def __init__(self):
+        n = 1 << self.order
+        self.op_bytes = {"c2c_fwd": 16 * n, "c2c_bwd": 16 * n}
+        self.bytes_per_step = sum(self.op_bytes.values())
+        self.dominant = "c2c_fwd"
+        self.host_in = None
+
+    def setup(self, device):
+        import torch
+        import zldsp_fft_b200 as Z
+        self.Z = Z
+        n = 1 << self.order
+        rng = np.random.default_rng(1001)
+        x = (rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)).astype(np.complex64)
+        self.host_x = x
+        self.plan = Z.Plan(Z.C2C, self.order, np.float32, device=device)
+        self.A = torch.from_numpy(x.view(np.float32).copy()).to(device)
+        self.B = torch.empty_like(self.A)
+        self.C = torch.empty_like(self.A)
+        self.flush_buf = torch.empty(64 << 20, dtype=torch.float32, device=device)
+        # Each direction recorded into a CUDA graph (one kernel each), so the
+        # timed op is the device's own latency, not the host's enqueue time.
+        p = self.plan
+        fwd = lambda st: p.exec_device(Z.FORWARD, Z.AOS, Z.AOS, self.A.data_ptr(), None,  # noqa: E731
+                                       self.B.data_ptr(), None, 1, stream=st)
+        bwd = lambda st: p.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, self.B.data_ptr(), None,  # noqa: E731
+                                       self.C.data_ptr(), None, 1, stream=st)
+        s = torch.cuda.Stream(device)
+        with torch.cuda.stream(s):
+            fwd(s.cuda_stream)
+            bwd(s.cuda_stream)
+        torch.cuda.synchronize(device)
+        self.graphs = {}
+        for name, fn in (("c2c_fwd", fwd), ("c2c_bwd", bwd)):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                fn(s.cuda_stream)
+            self.graphs[name] = g
+        torch.cuda.synchronize(device)
+
+    def flush(self, st):
+        self.flush_buf.fill_(1.0)
+
+    def ops(self, step):
+        return [(name, lambda st, g=g: g.replay()) for name, g in self.graphs.items()]
+
+    def take_launches(self):
+        return self.plan.take_launch_count()
+
+    def compare(self, stream, reps):
+        """Microseconds per transform and the error of forward (vs numpy FP64)
+        and of the round trip (backward(forward(x)) / N vs x)."""
+        x = self.host_x.astype(np.complex128)
+        y = self.B.cpu().numpy().view(np.complex64)
+        z = self.C.cpu().numpy().view(np.complex64)
+        ref = np.fft.fft(x)
+        n = 1 << self.order
+        return {
+            "fwd_rel_l2_vs_fp64": float(np.linalg.norm(y - ref) / np.linalg.norm(ref)),
+            "roundtrip_rel_l2": float(np.linalg.norm(z / n - x) / np.linalg.norm(x)),
+            "tolerance": 4 * self.order * 2.0 ** -24,
+        }
+
+    def cpu_sample_desc(self, frames):
+        return f"{frames} repetitions of the single forward+backward transform in one call, one thread, median of 3"
+
+    def setup_e2e(self):
+        import torch
+        n = 1 << self.order
+        self.hA = torch.from_numpy(self.host_x.view(np.float32).copy()).pin_memory()
+        self.hB = torch.empty_like(self.hA).pin_memory()
+        self.e2e_h2d = 2 * 8 * n
+        self.e2e_d2h = 2 * 8 * n
+
+    def e2e_step(self):
+        Z, p = self.Z, self.plan
+        p.exec_host(Z.FORWARD, Z.AOS, Z.AOS, self.hA.data_ptr(), None, self.hB.data_ptr(), None, 1)
+        p.exec_host(Z.BACKWARD, Z.AOS, Z.AOS, self.hB.data_ptr(), None, self.hB.data_ptr(), None, 1)
+
+    def cpu_run(self, frames, threads, kind):
+        from oracle import oracle as O
+        n = 1 << self.order
+        rng = np.random.default_rng(1001)
+        x = (rng.uniform(-1, 1, (1, n)) + 1j * rng.uniform(-1, 1, (1, n))).astype(np.complex64)
+        reps = max(1, frames)
+        if kind == "reference":
+            plan = O.RefPlan("c2c", self.order, "f32", 1)
+            t0 = time.perf_counter()
+            plan.cfft_roundtrip_repeat(x[0], reps)
+            dt = time.perf_counter() - t0
+            plan.close()
+        else:
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                O.cfft_port(O.cfft_port(x, True), False)
+            dt = time.perf_counter() - t0
+        return 2 * 16 * n * reps, dt
+
+    batch_for_cpu = 1 << 30  # repetitions the CPU sample may grow to
+    cpu_threads = 1          # one transform: the reference runs it on one thread
+
+
+WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G, "mixed": Mixed, "cfft64": Cfft64, "cfft10": Cfft10}
 
 
 # ------------------------------------------------------------------ CPU baseline
@@ -516,9 +747,9 @@ def cpu_baseline(wl, target_s=3.0, threads=None, kind=None):
     from oracle import oracle as O
     if kind is None:
         kind = "reference" if O.ref_available() else "port"
-    threads = threads or (os.cpu_count() or 1) if kind == "reference" else 1
-    frames = 64 if wl.host_in is None else 64
-    avail = wl.batch if wl.host_in is None else wl.host_in.shape[0]
+    threads = threads or getattr(wl, "cpu_threads", None) or (os.cpu_count() or 1) if kind == "reference" else 1
+    frames = 64
+    avail = getattr(wl, "batch_for_cpu", wl.batch) if wl.host_in is None else wl.host_in.shape[0]
     nbytes, dt = wl.cpu_run(frames, threads, kind)
     while dt < target_s / 4 and frames < avail:
         frames = min(avail, frames * 4)
@@ -541,9 +772,9 @@ def run_reference_arm(args, wl_cls):
     wl = wl_cls()
     from oracle import oracle as O
     kind = "reference" if O.ref_available() else "port"
-    threads = os.cpu_count() or 1
+    threads = getattr(wl, "cpu_threads", None) or os.cpu_count() or 1
     wl.host_in = hann_frames(min(wl.batch, 2048), wl.n, 1002) if hasattr(wl, "n") else None
-    avail = wl.host_in.shape[0] if wl.host_in is not None else wl.batch
+    avail = wl.host_in.shape[0] if wl.host_in is not None else getattr(wl, "batch_for_cpu", wl.batch)
     # each step: a bounded sample of the workload on all host cores
     frames = 16
     _, dt = wl.cpu_run(frames, threads, kind)
@@ -610,7 +841,10 @@ def run_ours(args, wl_cls):
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     t_start.record(stream)
+    flush = getattr(wl, "flush", None)
     for s in range(args.steps):
+        if flush is not None:
+            flush(st)  # outside the op events
         ops = wl.ops(s)
         ev[s][0].record(stream)
         for i, (_, fn) in enumerate(ops):
@@ -622,6 +856,8 @@ def run_ours(args, wl_cls):
     barrier()
     launches = wl.take_launches()
     elapsed_ms = t_start.elapsed_time(t_end)
+    if flush is not None:  # the steps' own time, without the flushes between them
+        elapsed_ms = sum(ev[s][0].elapsed_time(ev[s][-1]) for s in range(args.steps))
     per_op_ms = {name: statistics.mean(ev[s][i].elapsed_time(ev[s][i + 1]) for s in range(args.steps))
                  for i, name in enumerate(names)}
     if dist is not None:
@@ -664,6 +900,7 @@ def run_ours(args, wl_cls):
                      "kernel": dom, "algorithmic_bytes_per_launch": wl.op_bytes[dom],
                      "traffic": traffic},
         "per_op_gbs": {k: round(wl.op_bytes[k] / (v / 1e3) / 1e9, 1) for k, v in per_op_ms.items()},
+        "per_op_us": {k: round(v * 1e3, 2) for k, v in per_op_ms.items()},
         "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": wl.e2e_h2d,
                 "d2h_bytes_per_step": wl.e2e_d2h, "api": "zlfft_exec_host_batched, pinned host buffers"},
         "gpu_launches": launches,

@@ -171,6 +171,13 @@ ZLFFT_API int zlfft_plan_device_status(zlfft_plan plan, int* status);
  * as designed). The GPU context stays usable. No reference counterpart. */
 ZLFFT_API int zlfft_selftest_bounded_wait(int device, int* status);
 
+/* Tensor-core self-test: 128 independent 16-point forward DFTs of
+ * host_in (128 x 16 interleaved complex FP32) computed by one CTA with
+ * tcgen05 MMAs on split FP16 hi/lo operands accumulated in FP32 (the
+ * building block of the ZLFFT_MODE_TC_FP16 form); results to host_out, the
+ * device error word to *status. No reference counterpart. */
+ZLFFT_API int zlfft_selftest_tc_dft16(int device, const float* host_in, float* host_out, int* status);
+
 /* ---------------------------------------------------------------- mixed batches
  * Many transforms of different orders and kinds in one call. No reference
  * counterpart: the reference runs one CFFT<F>/RFFT<F> object per length

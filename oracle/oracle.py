@@ -77,6 +77,7 @@ def ref_lib():
         lib.zlref_cfft_exec.argtypes = [_c.c_int, _vp, _c.c_int, _c.c_int, _vp, _vp, _c.c_int, _vp, _vp, _sz]
         lib.zlref_rfft_exec.argtypes = [_c.c_int, _vp, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _sz]
         lib.zlref_switch_order.argtypes = [_c.c_int, _c.POINTER(_sz), _c.POINTER(_sz)]
+        lib.zlref_cfft_roundtrip_repeat.argtypes = [_c.c_int, _vp, _vp, _vp, _vp, _sz]
         _ref = lib
     return _ref
 
@@ -191,6 +192,15 @@ class RefPlan:
 
     def __del__(self):
         self.close()
+
+    def cfft_roundtrip_repeat(self, x, reps):
+        """forward then backward of the single AoS transform x, reps times on
+        one thread; returns the backward output of the last repetition."""
+        x = np.ascontiguousarray(x)
+        mid, out = np.empty_like(x), np.empty_like(x)
+        self.lib.zlref_cfft_roundtrip_repeat(self.prec, self.handle, x.ctypes.data, mid.ctypes.data,
+                                             out.ctypes.data, int(reps))
+        return out
 
     def cfft(self, x, forward=True, in_layout=AOS, out_layout=AOS, out=None):
         """x: (batch, N) complex (AoS) or a pair (re, im) of (batch, N) real arrays (SoA)."""

@@ -137,6 +137,20 @@ void rfft_exec(void* plan_v, int mode, int layout, const void* a_re, const void*
     });
 }
 
+// Latency loop: forward(in -> mid) then backward(mid -> out) of one AoS
+// transform, `reps` times, on the calling thread (the reference's own
+// single-transform use, without a foreign-call round trip per transform).
+template <typename F>
+void cfft_roundtrip_repeat(void* plan_v, const void* in, void* mid, void* out, size_t reps) {
+    auto* plan = static_cast<RefPlan<F>*>(plan_v);
+    using C = std::complex<F>;
+    auto& fft = *plan->cfft[0];
+    for (size_t r = 0; r < reps; ++r) {
+        fft.forward(const_cast<C*>(static_cast<const C*>(in)), static_cast<C*>(mid));
+        fft.backward(static_cast<C*>(mid), static_cast<C*>(out));
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -161,6 +175,11 @@ void zlref_rfft_exec(int prec, void* plan, int mode, int layout, const void* a_r
                      void* b_im, size_t batch) {
     if (prec == 0) rfft_exec<float>(plan, mode, layout, a_re, a_im, b_re, b_im, batch);
     else rfft_exec<double>(plan, mode, layout, a_re, a_im, b_re, b_im, batch);
+}
+
+void zlref_cfft_roundtrip_repeat(int prec, void* plan, const void* in, void* mid, void* out, size_t reps) {
+    if (prec == 0) cfft_roundtrip_repeat<float>(plan, in, mid, out, reps);
+    else cfft_roundtrip_repeat<double>(plan, in, mid, out, reps);
 }
 
 // The reference's algorithm switch on this host (src/common/zldsp_fft_common_system.hpp:132-157).

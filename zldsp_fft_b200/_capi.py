@@ -50,6 +50,7 @@ EXPORTS = (
     "zlfft_plan_copy_twiddles",
     "zlfft_plan_device_status",
     "zlfft_selftest_bounded_wait",
+    "zlfft_selftest_tc_dft16",
     "zlfft_mixed_create",
     "zlfft_mixed_exec",
     "zlfft_mixed_take_launch_count",
@@ -96,6 +97,7 @@ def lib() -> ctypes.CDLL:
         L.zlfft_plan_copy_twiddles.argtypes = [vp, vp, sz, ctypes.POINTER(sz)]
         L.zlfft_plan_device_status.argtypes = [vp, ctypes.POINTER(i)]
         L.zlfft_selftest_bounded_wait.argtypes = [i, ctypes.POINTER(i)]
+        L.zlfft_selftest_tc_dft16.argtypes = [i, vp, vp, ctypes.POINTER(i)]
         L.zlfft_mixed_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(Desc), sz, i]
         L.zlfft_mixed_exec.argtypes = [vp, i, vp]
         L.zlfft_mixed_take_launch_count.argtypes = [vp, ctypes.POINTER(sz)]

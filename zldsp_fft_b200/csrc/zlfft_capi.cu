@@ -114,6 +114,12 @@ __global__ void selftest_wait_kernel(int* err, uint32_t limit) {
     if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(err, zlfft::kDevErrWaitTimeout);
 }
 
+}  // namespace
+namespace zlfft {
+cudaError_t tc_selftest_launch(const float2* in, float2* out, const float2* tw16, int* err, cudaStream_t st);
+}
+namespace {
+
 struct TablesHolder {
     zlfft::TileTable f32{};
     zlfft::TileTable f64{};
@@ -1343,6 +1349,35 @@ int zlfft_exec_mixed_device(const zlfft_desc* descs, size_t n, void* stream) {
     }
     mixed_release(m);
     return rc;
+}
+
+int zlfft_selftest_tc_dft16(int device, const float* host_in, float* host_out, int* status) {
+    if (!host_in || !host_out || !status) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    DeviceGuard g(device);
+    const size_t bytes = 128 * 16 * sizeof(float2);
+    float2 tw[16];
+    for (int t = 0; t < 16; ++t) {
+        const double a = -2.0 * 3.141592653589793 * t / 16.0;
+        tw[t] = make_float2((float)cos(a), (float)sin(a));
+    }
+    void* d = nullptr;
+    ZL_CUDA(cudaMalloc(&d, 2 * bytes + sizeof(tw) + 256));
+    char* base = static_cast<char*>(d);
+    float2* din = reinterpret_cast<float2*>(base);
+    float2* dout = reinterpret_cast<float2*>(base + bytes);
+    float2* dtw = reinterpret_cast<float2*>(base + 2 * bytes);
+    int* derr = reinterpret_cast<int*>(base + 2 * bytes + sizeof(tw));
+    cudaError_t e = cudaMemcpy(din, host_in, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dtw, tw, sizeof(tw), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(derr, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(dout, 0, bytes);
+    if (e == cudaSuccess) e = zlfft::tc_selftest_launch(din, dout, dtw, derr, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(host_out, dout, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(status, derr, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "tensor-core self-test");
+    return ZLFFT_OK;
 }
 
 const char* zlfft_last_error(void) { return g_last_error.c_str(); }

@@ -36,7 +36,7 @@ template <typename F, int OP, int P>
 __device__ __forceinline__ bool mixed_try(int code, const MixedGroup& g, int tile, unsigned char* smem) {
     if (code != mixed_code(OP, P)) return false;
     TileWorker<F, P, OP, kAoS, kAoS, kMixedBlock, true> w(g.a, smem);
-    w.run(g.a, tile, nullptr, []() {});
+    w.run(g.a, tile, false, []() {});
     return true;
 }
 

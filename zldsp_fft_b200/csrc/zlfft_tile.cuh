@@ -409,11 +409,12 @@ struct TileWorker {
 
     __device__ __forceinline__ uint32_t sidx(int pos) const { return swz<C>(sbase + (uint32_t)pos); }
 
-    // Process tile `tile`. With a staging buffer, group 0 reads this tile's
-    // input from it (placed there by TMA) and calls refill() once done.
+    // Process tile `tile`. With use_tma, group 0 reads this tile's input from
+    // the staging buffer that follows the exchange buffer in shared memory
+    // (placed there by TMA) and calls refill() once done.
     template <class Refill>
-    __device__ __forceinline__ void run(const TileArgs& a, long long tile, const C* stage, Refill&& refill) {
-        const bool use_tma = stage != nullptr;
+    __device__ __forceinline__ void run(const TileArgs& a, long long tile, bool use_tma, Refill&& refill) {
+        const C* stage = sm + (size_t)TPC * N;
         const long long tr = tile * TPC + slot;
         const bool valid = tr < a.batch;
         // this slot's transform: contiguous (base + stride) or gathered pointers
@@ -724,7 +725,7 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
                 phase ^= 1u;
             }
         }
-        w.run(a, tile, use_tma ? stage : nullptr, [&]() {
+        w.run(a, tile, use_tma, [&]() {
             fence_proxy_async_smem();  // reads of the staging buffer before its TMA refill
             __syncthreads();           // staging fully read: refill it with the next tile
             issue(tile + gridDim.x);
