@@ -270,8 +270,11 @@ class Cfft2G:
     total = 1 << 28  # complex elements per order (2 GiB)
     dtype = "f32"
 
-    def __init__(self, total_log2=28):
+    def __init__(self, total_log2=28, form="plain"):
         self.total = 1 << total_log2
+        self.form = form
+        if form == "tc":
+            self.desc = self.desc + ", tensor-core split FP16 hi/lo form"
         self.op_bytes = {}
         for o in self.orders:
             for d in ("fwd", "bwd"):
@@ -283,7 +286,8 @@ class Cfft2G:
         import torch
         import zldsp_fft_b200 as Z
         self.Z = Z
-        self.plans = {o: Z.Plan(Z.C2C, o, np.float32, device=device) for o in self.orders}
+        mode = Z.MODE_TC_FP16 if self.form == "tc" else Z.MODE_PLAIN
+        self.plans = {o: Z.Plan(Z.C2C, o, np.float32, mode=mode, device=device) for o in self.orders}
         g = torch.Generator(device=device)
         g.manual_seed(1003)
         # A: input (never overwritten), B: forward output, C: backward output
@@ -311,6 +315,44 @@ class Cfft2G:
 
     def take_launches(self):
         return sum(p.take_launch_count() for p in self.plans.values())
+
+    def compare(self, stream, reps):
+        """Both forms at every order: GB/s of forward+backward and the relative
+        L2 error of forward against numpy's FP64 FFT on 8 transforms."""
+        import torch
+        Z = self.Z
+        out = {}
+        for form, mode in (("plain", Z.MODE_PLAIN), ("tc_fp16", Z.MODE_TC_FP16)):
+            res = {}
+            for o in self.orders:
+                p = Z.Plan(Z.C2C, o, np.float32, mode=mode, device=self.A.device.index)
+                b = self.total >> o
+
+                def step():
+                    p.exec_device(Z.FORWARD, Z.AOS, Z.AOS, self.A.data_ptr(), None, self.B.data_ptr(), None, b,
+                                  stream=stream.cuda_stream)
+                    p.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, self.B.data_ptr(), None, self.C.data_ptr(), None, b,
+                                  stream=stream.cuda_stream)
+                for _ in range(2):
+                    step()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):
+                    step()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+                n = 1 << o
+                k = min(8, b)
+                x = self.A[:k * n].cpu().numpy().astype(np.float64).view(np.complex128).reshape(k, n)
+                y = self.B[:k * n].cpu().numpy().astype(np.float64).view(np.complex128).reshape(k, n)
+                ref = np.fft.fft(x, axis=-1)
+                err = np.linalg.norm(y - ref, axis=-1) / np.linalg.norm(ref, axis=-1)
+                res[f"order{o}"] = {"gbs": round(2 * 16 * self.total / (ms / 1e3) / 1e9, 1),
+                                    "max_rel_l2": float(err.max()), "tolerance": 4 * o * 2.0 ** -24}
+            out[form] = res
+        return out
 
     batch = 1 << 14  # largest per-order batch (order 14), for sample sizing
 
@@ -892,7 +934,10 @@ def run_ours(args, wl_cls):
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic",
-        "config": {"workload": wl.desc, "form": "plain FP32 (reference's Stockham radix-4/8 DIT, CUDA cores)",
+        "config": {"workload": wl.desc,
+                   "form": ("tensor-core split FP16 hi/lo, FP32 accumulate (256-point passes), plain FP32 elsewhere"
+                            if getattr(wl, "form", "plain") == "tc" else
+                            "plain FP32 (reference's Stockham radix-4/8 DIT, CUDA cores)"),
                    "l2": getattr(wl, "l2", "rotating input/output sets, each step > 2x L2 (no L2 flush needed)"),
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -928,14 +973,17 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cfft2g")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--form", choices=["plain", "tc"], default="plain",
+                    help="cfft2g only: the plain FP32 form or the tensor-core split FP16 hi/lo form")
     ap.add_argument("--total-log2", type=int, default=None,
                     help="cfft2g only: complex elements per order = 2^k (default 28 = 2 GiB); smaller cases "
                          "are for profiling and are not the benchmark configuration")
     args = ap.parse_args()
     wl_cls = WORKLOADS[args.workload]
-    if args.total_log2 is not None:
+    if args.workload == "cfft2g" and (args.total_log2 is not None or args.form != "plain"):
         base = wl_cls
-        wl_cls = lambda: base(total_log2=args.total_log2)  # noqa: E731
+        tl = args.total_log2 if args.total_log2 is not None else 28
+        wl_cls = lambda: base(total_log2=tl, form=args.form)  # noqa: E731
         wl_cls.__name__ = base.__name__
     if args.impl == "reference":
         return run_reference_arm(args, wl_cls)

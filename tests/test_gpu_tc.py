@@ -24,3 +24,62 @@ def test_tc_dft16_selftest_matches_fp64():
     err = np.linalg.norm(out - ref, axis=1) / np.linalg.norm(ref, axis=1)
     # one radix-16 stage: 4 * log2(16) * 2^-24 is the per-transform FP32 bar
     assert err.max() <= 4 * 4 * 2.0 ** -24, err.max()
+
+
+def _c2c(plan, x, forward=True):
+    from tests import gpu_util as G
+    return G.run_c2c(plan, x, forward)
+
+
+@pytest.mark.parametrize("order", [14, 15, 16, 17, 18, 20])
+def test_tc_fp16_cfft_within_fp32_tolerance(oracle, order):
+    """CFFT<float> in the split-precision tensor-core form, forward and
+    backward, against the FP64 oracle with the FP32 bar 4 log2(N) 2^-24; the
+    form really runs (its results differ in rounding from the plain form's)."""
+    rng = np.random.default_rng(600 + order)
+    batch = 6 if order <= 16 else 2
+    n = 1 << order
+    x = (rng.uniform(-1, 1, (batch, n)) + 1j * rng.uniform(-1, 1, (batch, n))).astype(np.complex64)
+    tc = Z.Plan(Z.C2C, order, np.float32, mode=Z.MODE_TC_FP16)
+    plain = Z.Plan(Z.C2C, order, np.float32)
+    tol = oracle.tolerance(order, "f32")
+    y = _c2c(tc, x, True)
+    err = oracle.rel_l2(y, oracle.cfft_fp64(x))
+    assert err.max() <= tol, (err.max(), tol)
+    yp = _c2c(plain, x, True)
+    assert not np.array_equal(y, yp)
+    z = _c2c(tc, y, False)
+    err_b = oracle.rel_l2(z, oracle.cfft_fp64(y, False))
+    assert err_b.max() <= tol, (err_b.max(), tol)
+    assert tc.device_status() == 0
+
+
+def test_tc_fp16_extreme_magnitudes_and_chunks(oracle):
+    """Exact power-of-two scaling keeps the FP16 operands in range for inputs
+    of any FP32 magnitude; batches larger than one scratch chunk (two chunk
+    pipelines) and all-zero transforms come out right."""
+    rng = np.random.default_rng(7)
+    order, n = 14, 1 << 14
+    tc = Z.Plan(Z.C2C, order, np.float32, mode=Z.MODE_TC_FP16)
+    tol = oracle.tolerance(order, "f32")
+    base = (rng.uniform(-1, 1, (4, n)) + 1j * rng.uniform(-1, 1, (4, n)))
+    for scale in (1e-30, 1e-8, 1e12, 1e30):
+        x = (base * scale).astype(np.complex64)
+        y = _c2c(tc, x, True)
+        assert np.isfinite(y).all(), scale
+        assert oracle.rel_l2(y, oracle.cfft_fp64(x)).max() <= tol, scale
+    # 400 transforms > one 48 MiB chunk (384 of order 14): both chunk pipelines
+    x = (rng.uniform(-1, 1, (400, n)) + 1j * rng.uniform(-1, 1, (400, n))).astype(np.complex64)
+    x[17] = 0
+    y = _c2c(tc, x, True)
+    assert np.all(y[17] == 0)
+    keep = [i for i in range(400) if i != 17]
+    assert oracle.rel_l2(y[keep], oracle.cfft_fp64(x[keep])).max() <= tol
+
+
+def test_tc_mode_rejected_where_not_built():
+    h = ctypes.c_void_p()
+    lib = Z._capi.lib()
+    assert lib.zlfft_plan_create(ctypes.byref(h), Z.R2C, Z.F32, 12, Z.MODE_TC_FP16, -1) == Z._capi.ERR_UNSUPPORTED
+    assert lib.zlfft_plan_create(ctypes.byref(h), Z.C2C, Z.F64, 16, Z.MODE_TC_FP16, -1) == Z._capi.ERR_UNSUPPORTED
+    assert lib.zlfft_plan_create(ctypes.byref(h), Z.C2C, Z.F32, 16, Z.MODE_TC_BF16, -1) == Z._capi.ERR_UNSUPPORTED

@@ -100,6 +100,20 @@ __global__ void stage_table_kernel(zlfft::Cx<F>* tws, const zlfft::Cx<F>* tw, in
     tws[idx] = tw[q * k * (m / (4 * L))];
 }
 
+// Twiddles of one tensor-core pass with L_in > 1 (layout in zlfft_tc_pass.cuh),
+// copied from the unified table so the values are the ones the kernel would
+// otherwise read there.
+__global__ void tc_pass_table_kernel(float2* out, const float2* T, int n, int l_in) {
+    const int idx = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (idx < 4 * l_in) {
+        const uint32_t k = (uint32_t)(idx >> 2), b = (uint32_t)(idx & 3);
+        out[idx] = zlfft::tw_any(T, ((1u << b) * k) * (uint32_t)(n / (16 * l_in)), (uint32_t)n);
+    } else if (idx < 20 * l_in) {
+        const uint32_t r = (uint32_t)(idx - 4 * l_in), k = r >> 4, j = r & 15;
+        out[idx] = zlfft::tw_any(T, (j * k) * (uint32_t)(n / (256 * l_in)), (uint32_t)n);
+    }
+}
+
 // Self-test of the bounded-wait path: one CTA waits on an mbarrier that no
 // one ever arrives at, with a short poll limit; the wait gives up, the kernel
 // records kDevErrWaitTimeout in the error word and returns normally.
@@ -127,7 +141,10 @@ struct TablesHolder {
     zlfft::PassTable p64{};
     zlfft::GatherTable g32{};
     zlfft::GatherTable g64{};
+    zlfft::TcPassTable tc{};
     TablesHolder() {
+        zlfft::fill_tc_pass_a(tc);
+        zlfft::fill_tc_pass_b(tc);
         zlfft::fill_gather_f32(g32);
         zlfft::fill_gather_f64(g64);
         zlfft::fill_tile_c2c_f32(f32);
@@ -161,6 +178,8 @@ struct zlfft_plan_s {
     size_t tw_count = 0;
     void* d_tws = nullptr;  // per-stage twiddle tables
     void* d_rw = nullptr;   // RFFT split twiddle pairs
+    void* d_tctw = nullptr;  // tensor-core pass twiddles (MODE_TC_FP16), one section per pass
+    size_t tctw_off[zlfft::kMaxPasses] = {0, 0, 0};  // element offset of each pass's section
     // host staging
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;
@@ -199,6 +218,7 @@ void release(zlfft_plan p) {
     if (p->d_tw) cudaFree(p->d_tw);
     if (p->d_tws) cudaFree(p->d_tws);
     if (p->d_rw) cudaFree(p->d_rw);
+    if (p->d_tctw) cudaFree(p->d_tctw);
     if (p->d_err) cudaFree(p->d_err);
     if (p->d_scratch) cudaFree(p->d_scratch);
     for (int i = 0; i < 2; ++i) {
@@ -317,6 +337,18 @@ cudaError_t launch_pre(const zlfft_plan_s* p, int in_layout, const void* i0, con
     return cudaGetLastError();
 }
 
+// Kernel of pass pi: the tensor-core split-precision pass where the plan asks
+// for it and one exists (256-point passes, FP32 AoS), else the plain pass.
+zlfft::PassLaunchFn pick_pass(const zlfft_plan_s* p, int pi, bool fwd, int li, int lo) {
+    const int P = p->cfft_order;
+    if (p->mode == ZLFFT_MODE_TC_FP16 && li == ZLFFT_AOS && lo == ZLFFT_AOS) {
+        zlfft::PassLaunchFn f = tables().tc.fn[P - zlfft::kPassMinP][pi][fwd ? 1 : 0];
+        if (f) return f;
+    }
+    const zlfft::PassTable& t = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
+    return t.fn[P - zlfft::kPassMinP][pi][fwd ? 1 : 0][li][lo];
+}
+
 // Orders above the tile kernel: chunks of transforms through 2-3 Stockham
 // passes (zlfft_pass.cuh); RFFT orders add the split (forward) or the
 // pre-step (backward) as a separate elementwise kernel on the N/2-point
@@ -397,6 +429,8 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
             pa.in_stride = src_stride;
             pa.batch = nb;
             pa.tws = p->d_tws;
+            pa.tw = p->d_tw;
+            pa.tctw = p->d_tctw ? static_cast<const char*>(p->d_tctw) + p->tctw_off[pi] * 2 * p->esize : nullptr;
             pa.err = p->d_err;
             if (gfirst) {
                 pa.gin0 = gi0;
@@ -421,7 +455,7 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
             }
             const int li = pi == 0 ? src_layout : ZLFFT_AOS;
             const int lo = (last && !r2c) ? ol : ZLFFT_AOS;
-            zlfft::PassLaunchFn fn = row[pi][fwd ? 1 : 0][li][lo];
+            zlfft::PassLaunchFn fn = pick_pass(p, pi, fwd, li, lo);
             if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no pass kernel for order %d", p->order);
             e = fn(pa, st, ctx);
             if (e != cudaSuccess) return cuda_fail(e, "pass launch");
@@ -616,6 +650,8 @@ int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layo
             pa.in_stride = src_stride;
             pa.batch = nb;
             pa.tws = p->d_tws;
+            pa.tw = p->d_tw;
+            pa.tctw = p->d_tctw ? static_cast<const char*>(p->d_tctw) + p->tctw_off[pi] * 2 * p->esize : nullptr;
             pa.err = p->d_err;
             const size_t eb = (pi == 0 && src_layout == ZLFFT_SOA) ? p->esize : cx;
             pa.tma = (aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
@@ -631,7 +667,7 @@ int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layo
             }
             const int li = pi == 0 ? src_layout : ZLFFT_AOS;
             const int lo = (last && !r2c) ? ol : ZLFFT_AOS;
-            zlfft::PassLaunchFn fn = row[pi][fwd ? 1 : 0][li][lo];
+            zlfft::PassLaunchFn fn = pick_pass(p, pi, fwd, li, lo);
             if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no pass kernel for order %d", p->order);
             e = fn(pa, st, ctx);
             if (e != cudaSuccess) return cuda_fail(e, "pass launch");
@@ -1118,7 +1154,10 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
     if (order > 30) return fail(ZLFFT_ERR_INVALID_ARG, "order %zu out of range", order);
     if (kind == ZLFFT_R2C && order < 1)
         return fail(ZLFFT_ERR_INVALID_ARG, "RFFT order must be >= 1 (the reference underflows at 0)");
-    if (mode != ZLFFT_MODE_PLAIN) return fail(ZLFFT_ERR_UNSUPPORTED, "mode %d not available", mode);
+    if (mode != ZLFFT_MODE_PLAIN && mode != ZLFFT_MODE_TC_FP16)
+        return fail(ZLFFT_ERR_UNSUPPORTED, "mode %d not available", mode);
+    if (mode == ZLFFT_MODE_TC_FP16 && (kind != ZLFFT_C2C || precision != ZLFFT_F32))
+        return fail(ZLFFT_ERR_UNSUPPORTED, "the tensor-core split form is built for CFFT<float>");
     const int cfft_order = kind == ZLFFT_C2C ? (int)order : (int)order - 1;
     if (cfft_order > zlfft::kPassMaxP) return fail(ZLFFT_ERR_UNSUPPORTED, "order %zu above the supported maximum", order);
 
@@ -1201,6 +1240,30 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
         else
             rfft_twiddle_kernel<double><<<blocks, 256, 0, p->stream>>>(static_cast<double2*>(p->d_rw), (int)order,
                                                                        cnt);
+    }
+    if (mode == ZLFFT_MODE_TC_FP16 && cfft_order >= zlfft::kPassMinP) {
+        // per-pass tables of the tensor-core passes with L_in > 1: 20 L_in entries each
+        size_t total = 0;
+        const auto& tt = tables().tc;
+        for (int pi = 0; pi < zlfft::kMaxPasses; ++pi) {
+            p->tctw_off[pi] = total;
+            const int l_in = tt.l_in[cfft_order - zlfft::kPassMinP][pi];
+            if (tt.fn[cfft_order - zlfft::kPassMinP][pi][0] && l_in > 1) total += 20 * (size_t)l_in;
+        }
+        if (total) {
+            if (cudaMalloc(&p->d_tctw, total * cx_bytes) != cudaSuccess) {
+                release(p);
+                return fail(ZLFFT_ERR_ALLOC, "tensor-core twiddle allocation failed");
+            }
+            for (int pi = 0; pi < zlfft::kMaxPasses; ++pi) {
+                const int l_in = tt.l_in[cfft_order - zlfft::kPassMinP][pi];
+                if (!tt.fn[cfft_order - zlfft::kPassMinP][pi][0] || l_in <= 1) continue;
+                const int cnt = 20 * l_in;
+                tc_pass_table_kernel<<<(cnt + 255) / 256, 256, 0, p->stream>>>(
+                    static_cast<float2*>(p->d_tctw) + p->tctw_off[pi], static_cast<const float2*>(p->d_tw), (int)m,
+                    l_in);
+            }
+        }
     }
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include "zlfft_pass.cuh"
+#include "zlfft_tc_pass.cuh"
 #include "zlfft_tile.cuh"
 
 namespace zlfft {
@@ -240,6 +241,83 @@ template <typename F, int Lo, int Hi>
 void fill_pass_range(PassTable& t) {
     fill_pass_range_impl<F, Lo, Hi>(t, std::make_integer_sequence<int, Hi - Lo + 1>{});
 }
+
+
+// ------------------------------------------------------------------ tensor-core passes
+// [order - kPassMinP][pass][fwd]: the split-precision kernel for the 256-point
+// passes of FP32 complex AoS data (null where a pass is not 256 points).
+struct TcPassTable {
+    PassLaunchFn fn[kPassMaxP - kPassMinP + 1][kMaxPasses][2];
+    int l_in[kPassMaxP - kPassMinP + 1][kMaxPasses];  // sub-length at the pass's entry
+};
+
+template <int P, int PI, bool FWD>
+cudaError_t launch_tc_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchCtx& ctx) {
+    using Cfg = TcPassCfg<P, PI>;
+    auto kern = tc_pass_kernel<P, PI, FWD>;
+    PassArgs a = a_in;
+    PassMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    static const bool tma_enabled = [] {
+        const char* e = getenv("ZLFFT_PASS_TMA");
+        return !(e && e[0] == '0');
+    }();
+    a.tma = (tma_enabled && a.tma && !(Cfg::FIRST && a.gin0) && encode_pass_maps<float, P, PI, kAoS>(a, maps)) ? 1
+                                                                                                                 : 0;
+    // Resident CTAs per SM from the kernel's own resources: registers and
+    // shared memory per CTA (1 KB of it reserved by the driver), with the
+    // shared-memory carve-out at its maximum. (The occupancy query answers 1
+    // for this kernel, which would leave two thirds of each SM idle.)
+    static const int blocks_per_sm = [kern]() {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncAttributes fa{};
+        int dev = 0, regs_sm = 65536, smem_sm = 228 * 1024;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        int b = 1;
+        if (cudaFuncGetAttributes(&fa, kern) == cudaSuccess && fa.numRegs > 0) {
+            const int by_regs = regs_sm / (fa.numRegs * Cfg::THREADS);
+            const int by_smem = smem_sm / (int)(Cfg::SMEM + 1024);
+            b = by_regs < by_smem ? by_regs : by_smem;
+            if (b < 1) b = 1;
+        }
+        return b;
+    }();
+    if (a.batch <= 0) return cudaSuccess;
+    const long long items = a.batch * Cfg::CPT;
+    const long long cap = (long long)ctx.num_sms * blocks_per_sm;
+    const unsigned grid = (unsigned)(items < cap ? items : cap);
+    kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(a, maps);
+    if (ctx.launches) ++*ctx.launches;
+    return cudaGetLastError();
+}
+
+template <int P, int PI>
+void fill_tc_pass_one(TcPassTable& t) {
+    t.l_in[P - kPassMinP][PI] = PassCfg<float, P, PI>::L_IN;
+    if constexpr (pass_radix(P, PI) == 256 && PassCfg<float, P, PI>::UPC == 16) {
+        t.fn[P - kPassMinP][PI][1] = launch_tc_pass<P, PI, true>;
+        t.fn[P - kPassMinP][PI][0] = launch_tc_pass<P, PI, false>;
+    } else {
+        t.fn[P - kPassMinP][PI][0] = t.fn[P - kPassMinP][PI][1] = nullptr;
+    }
+}
+
+template <int P>
+void fill_tc_pass_order(TcPassTable& t) {
+    fill_tc_pass_one<P, 0>(t);
+    fill_tc_pass_one<P, 1>(t);
+    if constexpr (pass_count(P) > 2) fill_tc_pass_one<P, 2>(t);
+}
+
+template <int Lo, int... Ps>
+void fill_tc_pass_range_impl(TcPassTable& t, std::integer_sequence<int, Ps...>) {
+    (fill_tc_pass_order<Lo + Ps>(t), ...);
+}
+void fill_tc_pass_a(TcPassTable& t);  // orders 14..18
+void fill_tc_pass_b(TcPassTable& t);  // orders 19..24
 
 // Each translation unit fills its part of a precision's table.
 void fill_tile_c2c_f32(TileTable& t);

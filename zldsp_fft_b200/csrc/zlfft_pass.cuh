@@ -104,6 +104,8 @@ struct PassArgs {
     long long in_stride;   // elements between transforms of the input
     long long out_stride;  // elements between transforms of the output
     const void* tws;       // per-stage twiddle tables (stage_l0 layout)
+    const void* tw;        // unified table T[t] = W_N^t, t < 3N/4 (tensor-core passes)
+    const void* tctw;      // this pass's tensor-core twiddles when L_in > 1 (zlfft_tc_pass.cuh)
     int* err;              // device error word (kDevErrWaitTimeout on a timed-out wait)
     int tma;               // the tensor maps describe the input (else direct loads)
     // Gathered transforms (mixed batches): the first pass reads transform t
