@@ -446,6 +446,12 @@ class Mixed:
         self.A = (torch.rand(self.in_total // 4, generator=g, device=device) * 2 - 1).contiguous()
         self.B = torch.zeros(self.out_total // 4, dtype=torch.float32, device=device)
         a, b = self.A.data_ptr(), self.B.data_ptr()
+        # autotuned plan per order (set-up, outside the timed region): the batch's
+        # plans are created in the tuned mode
+        Z.autotune(Z.C2C, 6, 16, np.float32, device=device)
+        Z.autotune(Z.R2C, 6, 16, np.float32, device=device)
+        self.tuning = {f"{'c2c' if k == Z.C2C else 'r2c'}{o}": Z.tuning(k, o, np.float32, device=device)
+                       for k in (Z.C2C, Z.R2C) for o in range(14, 17)}
         descs = [(Z.C2C if c else Z.R2C, int(o), Z.FORWARD, a + int(io), b + int(oo))
                  for c, o, io, oo in zip(self.is_c, self.orders, self.in_off, self.out_off)]
         self.mb = Z.MixedBatch(descs, np.float32, device=device)
@@ -498,6 +504,7 @@ class Mixed:
             worst = max(worst, float(np.linalg.norm(y - ref) / np.linalg.norm(ref)))
         out["max_rel_l2_vs_fp64"] = worst
         out["tolerance_order16"] = 4 * 16 * 2.0 ** -24
+        out["autotuned_multipass_plans"] = self.tuning
         return out
 
     def cpu_sample_desc(self, frames):

@@ -64,6 +64,7 @@ typedef struct zlfft_plan_s* zlfft_plan;
 #define ZLFFT_MODE_TC_FP16 1 /* radix-16 sub-DFTs on tensor cores, split hi/lo FP16 */
 #define ZLFFT_MODE_TC_BF16 2 /* split 3-way BF16 */
 #define ZLFFT_MODE_TC_TF32 3 /* 3xTF32 */
+#define ZLFFT_MODE_TUNED 4   /* the autotuned plan of this device and size (see zlfft_autotune) */
 
 /* Create a plan for one transform size.
  * Replaces the constructors CFFT<F>::CFFT(size_t order)
@@ -230,6 +231,51 @@ ZLFFT_API int zlfft_mixed_destroy(zlfft_mixed mixed);
 /* One-shot form: create, run with ZLFFT_SCHED_PERSISTENT on `stream`,
  * synchronise the stream, destroy. */
 ZLFFT_API int zlfft_exec_mixed_device(const zlfft_desc* descs, size_t n, void* stream);
+
+/* ---------------------------------------------------------------- autotuning
+ * No reference counterpart: the reference picks its algorithm from the host
+ * CPU's cache sizes (src/common/zldsp_fft_common_system.hpp:132-157); here the
+ * plan of each transform size is chosen by measurement on the device.
+ *
+ * Tuned parameters: for the multi-pass sizes (complex order >= 14) the scratch
+ * chunk per pipeline, one or two chunk pipelines, TMA staging or direct loads
+ * of the pass inputs, and for CFFT<float> the computation form (plain or the
+ * tensor-core split form); for the single-tile sizes, TMA staging or direct
+ * loads. None of them changes the arithmetic of a form. Every plan created
+ * afterwards on that device and size uses the tuned chunk, pipelines and
+ * staging; plans created with ZLFFT_MODE_TUNED also take the tuned form
+ * (without a tuning entry they behave as ZLFFT_MODE_PLAIN). Mixed batches
+ * create their plans with ZLFFT_MODE_TUNED. If the environment variable
+ * ZLFFT_TUNE_FILE names a file written by zlfft_tuning_save, the first plan
+ * created on a device loads it. */
+typedef struct zlfft_tuning {
+    int chunk_mb;       /* scratch per chunk pipeline buffer, MiB (0: single-tile size) */
+    int streams;        /* chunk pipelines, 1 or 2 */
+    int tma;            /* 1: inputs staged by TMA copies; 0: direct loads */
+    int form;           /* ZLFFT_MODE_PLAIN or ZLFFT_MODE_TC_FP16 */
+    double gbs;         /* measured algorithmic GB/s of the chosen plan (forward, AoS) */
+    double gbs_default; /* of the default plan (48 MiB, 2 pipelines, TMA, plain) */
+} zlfft_tuning;
+
+/* Measure the candidate plans of every order in [order_lo, order_hi] for
+ * (kind, precision) on `device` (-1: current), forward AoS -> AoS on about
+ * 512 MiB of device buffers allocated for the duration, and record the
+ * fastest in the process's tuning table (replacing older entries). Takes
+ * about a second per multi-pass order. */
+ZLFFT_API int zlfft_autotune(int device, int kind, int precision, size_t order_lo, size_t order_hi);
+
+/* The tuning entry of (device, kind, precision, order); ZLFFT_ERR_UNSUPPORTED
+ * if there is none. */
+ZLFFT_API int zlfft_tuning_get(int device, int kind, int precision, size_t order, zlfft_tuning* out);
+
+/* Write the device's tuning entries to a text file, headed by the GPU's name
+ * and SM count; load such a file into the table (entries written on a GPU of
+ * another name or SM count are skipped). *loaded = entries taken. */
+ZLFFT_API int zlfft_tuning_save(int device, const char* path);
+ZLFFT_API int zlfft_tuning_load(int device, const char* path, size_t* loaded);
+
+/* Forget every tuning entry of every device. */
+ZLFFT_API int zlfft_tuning_clear(void);
 
 /* Message of the calling thread's last failure ("" if none). */
 ZLFFT_API const char* zlfft_last_error(void);

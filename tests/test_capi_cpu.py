@@ -44,6 +44,18 @@ def test_invalid_arguments_rejected_without_cuda():
     assert lib.zlfft_plan_get_size(None, ctypes.byref(sz)) == C.ERR_INVALID_ARG
 
 
+def test_tuning_arguments_rejected_without_cuda():
+    lib = C.lib()
+    assert lib.zlfft_autotune(0, 7, C.F32, 10, 12) == C.ERR_INVALID_ARG
+    assert lib.zlfft_autotune(0, C.C2C, 9, 10, 12) == C.ERR_INVALID_ARG
+    assert lib.zlfft_autotune(0, C.C2C, C.F32, 12, 10) == C.ERR_UNSUPPORTED
+    assert lib.zlfft_autotune(0, C.R2C, C.F32, 0, 3) == C.ERR_UNSUPPORTED
+    assert lib.zlfft_tuning_get(0, C.C2C, C.F32, 10, None) == C.ERR_INVALID_ARG
+    assert lib.zlfft_tuning_save(0, None) == C.ERR_INVALID_ARG
+    assert lib.zlfft_tuning_load(0, None, None) == C.ERR_INVALID_ARG
+    assert lib.zlfft_tuning_clear() == C.OK
+
+
 def test_mixed_batch_descriptors_rejected_without_cuda():
     """zlfft_mixed_create checks every descriptor before it touches CUDA."""
     lib = C.lib()

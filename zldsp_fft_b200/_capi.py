@@ -26,7 +26,7 @@ C2C, R2C = 0, 1
 F32, F64 = 0, 1
 AOS, SOA = 0, 1
 FORWARD, BACKWARD, FORWARD_SQR_MAG = 0, 1, 2
-MODE_PLAIN, MODE_TC_FP16, MODE_TC_BF16, MODE_TC_TF32 = 0, 1, 2, 3
+MODE_PLAIN, MODE_TC_FP16, MODE_TC_BF16, MODE_TC_TF32, MODE_TUNED = 0, 1, 2, 3, 4
 SCHED_PER_ORDER, SCHED_PERSISTENT, SCHED_GRAPH = 0, 1, 2
 
 
@@ -34,6 +34,12 @@ class Desc(ctypes.Structure):
     """zlfft_desc: one transform of a mixed batch (device pointers)."""
     _fields_ = [("kind", ctypes.c_int), ("precision", ctypes.c_int), ("order", ctypes.c_int), ("op", ctypes.c_int),
                 ("in_", ctypes.c_void_p), ("out", ctypes.c_void_p)]
+
+
+class Tuning(ctypes.Structure):
+    """zlfft_tuning: the measured plan parameters of one transform size."""
+    _fields_ = [("chunk_mb", ctypes.c_int), ("streams", ctypes.c_int), ("tma", ctypes.c_int), ("form", ctypes.c_int),
+                ("gbs", ctypes.c_double), ("gbs_default", ctypes.c_double)]
 
 
 # every symbol include/zlfft.h declares
@@ -57,6 +63,11 @@ EXPORTS = (
     "zlfft_mixed_device_status",
     "zlfft_mixed_destroy",
     "zlfft_exec_mixed_device",
+    "zlfft_autotune",
+    "zlfft_tuning_get",
+    "zlfft_tuning_save",
+    "zlfft_tuning_load",
+    "zlfft_tuning_clear",
     "zlfft_last_error",
     "zlfft_version",
 )
@@ -104,6 +115,11 @@ def lib() -> ctypes.CDLL:
         L.zlfft_mixed_device_status.argtypes = [vp, ctypes.POINTER(i)]
         L.zlfft_mixed_destroy.argtypes = [vp]
         L.zlfft_exec_mixed_device.argtypes = [ctypes.POINTER(Desc), sz, vp]
+        L.zlfft_autotune.argtypes = [i, i, i, sz, sz]
+        L.zlfft_tuning_get.argtypes = [i, i, i, sz, ctypes.POINTER(Tuning)]
+        L.zlfft_tuning_save.argtypes = [i, ctypes.c_char_p]
+        L.zlfft_tuning_load.argtypes = [i, ctypes.c_char_p, ctypes.POINTER(sz)]
+        L.zlfft_tuning_clear.argtypes = []
         L.zlfft_last_error.restype = ctypes.c_char_p
         L.zlfft_last_error.argtypes = []
         L.zlfft_version.restype = ctypes.c_char_p

@@ -163,6 +163,87 @@ const TablesHolder& tables() {
     return t;
 }
 
+
+// ------------------------------------------------------------------ autotuning table
+// Process-wide: (device, kind, precision, order) -> the plan parameters that
+// measured fastest there (zlfft_autotune), or that a tuning file recorded.
+struct TuneEntry {
+    int chunk_mb = 48, streams = 2, tma = 1, form = ZLFFT_MODE_PLAIN;
+    double gbs = 0, gbs_default = 0;
+};
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, TuneEntry> g_tune;
+std::once_flag g_tune_env_once[64];
+
+bool tune_lookup(int device, int kind, int prec, int order, TuneEntry* e) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(std::make_tuple(device, kind, prec, order));
+    if (it == g_tune.end()) return false;
+    *e = it->second;
+    return true;
+}
+
+// GPU identity written into tuning files: name (spaces as '_') and SM count.
+int gpu_identity(int device, std::string* name, int* sms) {
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+    std::string n = prop.name;
+    for (char& c : n)
+        if (c == ' ' || c == '\t') c = '_';
+    *name = n;
+    *sms = prop.multiProcessorCount;
+    return ZLFFT_OK;
+}
+
+int tuning_load_impl(int device, const char* path, size_t* loaded) {
+    if (loaded) *loaded = 0;
+    FILE* f = fopen(path, "r");
+    if (!f) return fail(ZLFFT_ERR_INVALID_ARG, "cannot open tuning file %s", path);
+    std::string name;
+    int sms = 0;
+    int rc = gpu_identity(device, &name, &sms);
+    if (rc) {
+        fclose(f);
+        return rc;
+    }
+    char line[512];
+    bool same_gpu = false;
+    size_t n = 0;
+    while (fgets(line, sizeof(line), f)) {
+        char gname[256];
+        int gsms = 0;
+        if (sscanf(line, "gpu %255s sms %d", gname, &gsms) == 2) {
+            same_gpu = (name == gname && sms == gsms);
+            continue;
+        }
+        int kind, prec, order, chunk, streams, tma, form;
+        double gbs, gbs0;
+        if (sscanf(line, "entry %d %d %d %d %d %d %d %lf %lf", &kind, &prec, &order, &chunk, &streams, &tma, &form,
+                   &gbs, &gbs0) != 9)
+            continue;
+        if (!same_gpu) continue;
+        const bool ok = (kind == ZLFFT_C2C || kind == ZLFFT_R2C) && (prec == ZLFFT_F32 || prec == ZLFFT_F64) &&
+                        order >= 0 && order <= zlfft::kPassMaxP + 1 && chunk >= 0 && chunk <= 4096 &&
+                        (streams == 1 || streams == 2) && (tma == 0 || tma == 1) &&
+                        (form == ZLFFT_MODE_PLAIN ||
+                         (form == ZLFFT_MODE_TC_FP16 && kind == ZLFFT_C2C && prec == ZLFFT_F32));
+        if (!ok) continue;
+        TuneEntry e;
+        e.chunk_mb = chunk;
+        e.streams = streams;
+        e.tma = tma;
+        e.form = form;
+        e.gbs = gbs;
+        e.gbs_default = gbs0;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune[std::make_tuple(device, kind, prec, order)] = e;
+        ++n;
+    }
+    fclose(f);
+    if (loaded) *loaded = n;
+    return ZLFFT_OK;
+}
 }  // namespace
 
 struct zlfft_plan_s {
@@ -196,6 +277,11 @@ struct zlfft_plan_s {
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     size_t chunk = 0;  // transforms per chunk; intermediates of one chunk stay L2-resident
     int* d_err = nullptr;  // device error word written by kernels (bounded waits that ran out)
+    // plan parameters: defaults, or the device's tuning entry for this size
+    size_t chunk_mb = 48;   // scratch per chunk-pipeline buffer (measured plateau: 32-128 MiB)
+    int nlanes = 2;         // chunk pipelines
+    int use_tma = 1;        // TMA staging of kernel inputs (else direct loads)
+    bool tc_form = false;   // 256-point passes in the tensor-core split form
     std::mutex mu;
 };
 
@@ -276,7 +362,7 @@ int ensure_scratch(zlfft_plan_s* p) {
     const size_t cx = 2 * p->esize;
     const size_t n = size_t{1} << p->cfft_order;
     const size_t per = n * cx;
-    size_t budget = size_t{48} << 20;  // bytes of one scratch buffer (measured plateau: 32-128 MiB)
+    size_t budget = p->chunk_mb << 20;  // bytes of one scratch buffer
     if (const char* env = getenv("ZLFFT_CHUNK_MB")) {
         const long v = atol(env);
         if (v > 0) budget = (size_t)v << 20;
@@ -341,7 +427,7 @@ cudaError_t launch_pre(const zlfft_plan_s* p, int in_layout, const void* i0, con
 // for it and one exists (256-point passes, FP32 AoS), else the plain pass.
 zlfft::PassLaunchFn pick_pass(const zlfft_plan_s* p, int pi, bool fwd, int li, int lo) {
     const int P = p->cfft_order;
-    if (p->mode == ZLFFT_MODE_TC_FP16 && li == ZLFFT_AOS && lo == ZLFFT_AOS) {
+    if (p->tc_form && li == ZLFFT_AOS && lo == ZLFFT_AOS) {
         zlfft::PassLaunchFn f = tables().tc.fn[P - zlfft::kPassMinP][pi][fwd ? 1 : 0];
         if (f) return f;
     }
@@ -379,7 +465,7 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
     // back to) the caller's stream, so one chunk's passes overlap the other's
     // launch gaps and wave tails. Each stream owns two scratch buffers.
     const long long nchunks = (a.batch + (long long)p->chunk - 1) / (long long)p->chunk;
-    const bool fork = nchunks > 1;
+    const bool fork = nchunks > 1 && p->nlanes > 1;
     if (fork) {
         if (cudaEventRecord(p->ev_fork, st) != cudaSuccess) return fail(ZLFFT_ERR_CUDA, "event record failed");
         for (int i = 0; i < 2; ++i)
@@ -439,7 +525,7 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
             {
                 // bulk-copy rows need 16-byte aligned sources (bases and transform stride)
                 const size_t eb = (pi == 0 && src_layout == ZLFFT_SOA) ? p->esize : cx;
-                pa.tma = (!gfirst && aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
+                pa.tma = (p->use_tma && !gfirst && aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
                           (nb == 1 || ((size_t)src_stride * eb) % 16 == 0)) ? 1 : 0;
             }
             if (last && !r2c) {
@@ -531,7 +617,7 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
         const size_t in_elem_bytes = in_soa ? p->esize : 2 * p->esize;  // complex or pairs of reals
         const bool al = aligned(in0, 16) && (!in_soa || aligned(in1, 16)) &&
                         (batch == 1 || ((size_t)a.in_stride * in_elem_bytes) % 16 == 0);
-        a.tma = al ? 1 : 0;
+        a.tma = (al && p->use_tma) ? 1 : 0;
     }
 
     const int dop = device_op_code(p, op);
@@ -654,7 +740,7 @@ int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layo
             pa.tctw = p->d_tctw ? static_cast<const char*>(p->d_tctw) + p->tctw_off[pi] * 2 * p->esize : nullptr;
             pa.err = p->d_err;
             const size_t eb = (pi == 0 && src_layout == ZLFFT_SOA) ? p->esize : cx;
-            pa.tma = (aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
+            pa.tma = (p->use_tma && aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
                       (nb == 1 || ((size_t)src_stride * eb) % 16 == 0)) ? 1 : 0;
             if (last && !r2c) {
                 pa.out0 = uo0;
@@ -1014,7 +1100,8 @@ int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int d
             auto it = plan_of.find(key);
             if (it == plan_of.end()) {
                 zlfft_plan p = nullptr;
-                int rc = zlfft_plan_create(&p, d.kind, d.precision, (size_t)d.order, ZLFFT_MODE_PLAIN, device);
+                // the device's autotuned plan for this size where there is one
+                int rc = zlfft_plan_create(&p, d.kind, d.precision, (size_t)d.order, ZLFFT_MODE_TUNED, device);
                 if (rc) {
                     mixed_release(m);
                     return rc;
@@ -1154,7 +1241,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
     if (order > 30) return fail(ZLFFT_ERR_INVALID_ARG, "order %zu out of range", order);
     if (kind == ZLFFT_R2C && order < 1)
         return fail(ZLFFT_ERR_INVALID_ARG, "RFFT order must be >= 1 (the reference underflows at 0)");
-    if (mode != ZLFFT_MODE_PLAIN && mode != ZLFFT_MODE_TC_FP16)
+    if (mode != ZLFFT_MODE_PLAIN && mode != ZLFFT_MODE_TC_FP16 && mode != ZLFFT_MODE_TUNED)
         return fail(ZLFFT_ERR_UNSUPPORTED, "mode %d not available", mode);
     if (mode == ZLFFT_MODE_TC_FP16 && (kind != ZLFFT_C2C || precision != ZLFFT_F32))
         return fail(ZLFFT_ERR_UNSUPPORTED, "the tensor-core split form is built for CFFT<float>");
@@ -1176,6 +1263,21 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
     }
     p->device = device;
     DeviceGuard g(device);
+    if (device >= 0 && device < 64) {
+        std::call_once(g_tune_env_once[device], [device]() {
+            if (const char* path = getenv("ZLFFT_TUNE_FILE")) tuning_load_impl(device, path, nullptr);
+        });
+    }
+    {
+        TuneEntry te;
+        if (tune_lookup(device, kind, precision, (int)order, &te)) {
+            if (te.chunk_mb > 0) p->chunk_mb = (size_t)te.chunk_mb;
+            p->nlanes = te.streams;
+            p->use_tma = te.tma;
+            if (mode == ZLFFT_MODE_TUNED && te.form == ZLFFT_MODE_TC_FP16) p->tc_form = true;
+        }
+        if (mode == ZLFFT_MODE_TC_FP16) p->tc_form = true;
+    }
     cudaError_t e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
         release(p);
@@ -1241,7 +1343,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
             rfft_twiddle_kernel<double><<<blocks, 256, 0, p->stream>>>(static_cast<double2*>(p->d_rw), (int)order,
                                                                        cnt);
     }
-    if (mode == ZLFFT_MODE_TC_FP16 && cfft_order >= zlfft::kPassMinP) {
+    if (p->tc_form && cfft_order >= zlfft::kPassMinP) {
         // per-pass tables of the tensor-core passes with L_in > 1: 20 L_in entries each
         size_t total = 0;
         const auto& tt = tables().tc;
@@ -1446,5 +1548,188 @@ int zlfft_selftest_tc_dft16(int device, const float* host_in, float* host_out, i
 const char* zlfft_last_error(void) { return g_last_error.c_str(); }
 
 const char* zlfft_version(void) { return "zlfft-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"
+
+namespace {
+
+// One candidate plan timed on `batch` transforms: forward AoS -> AoS.
+int time_candidate(int device, int kind, int prec, int order, const TuneEntry& c, const void* in, void* out,
+                   size_t batch, cudaStream_t st, double* ms) {
+    zlfft_plan p = nullptr;
+    int rc = zlfft_plan_create(&p, kind, prec, (size_t)order, c.form, device);
+    if (rc) return rc;
+    p->chunk_mb = c.chunk_mb > 0 ? (size_t)c.chunk_mb : p->chunk_mb;
+    p->nlanes = c.streams;
+    p->use_tma = c.tma;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    constexpr int kReps = 5;
+    for (int i = 0; i < 2 && !rc; ++i)
+        rc = exec_device_impl(p, ZLFFT_FORWARD, ZLFFT_AOS, ZLFFT_AOS, in, nullptr, out, nullptr, batch, 0, 0, st);
+    if (!rc) {
+        cudaEventRecord(e0, st);
+        for (int i = 0; i < kReps && !rc; ++i)
+            rc = exec_device_impl(p, ZLFFT_FORWARD, ZLFFT_AOS, ZLFFT_AOS, in, nullptr, out, nullptr, batch, 0, 0, st);
+        cudaEventRecord(e1, st);
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    float t = 0;
+    if (!rc && e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int st_err = 0;
+    cudaMemcpy(&st_err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    release(p);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "autotune timing");
+    if (st_err) return fail(ZLFFT_ERR_DEVICE_TIMEOUT, "a device-side wait ran out during autotuning");
+    *ms = t / kReps;
+    return ZLFFT_OK;
+}
+
+int autotune_impl(int device, int kind, int prec, size_t lo, size_t hi) {
+    if (kind != ZLFFT_C2C && kind != ZLFFT_R2C) return fail(ZLFFT_ERR_INVALID_ARG, "invalid kind %d", kind);
+    if (prec != ZLFFT_F32 && prec != ZLFFT_F64) return fail(ZLFFT_ERR_INVALID_ARG, "invalid precision %d", prec);
+    const size_t min_order = kind == ZLFFT_R2C ? 1 : 0;
+    const size_t max_order = (size_t)zlfft::kPassMaxP + (kind == ZLFFT_R2C ? 1 : 0);
+    if (lo < min_order || hi > max_order || lo > hi)
+        return fail(ZLFFT_ERR_UNSUPPORTED, "orders %zu..%zu outside %zu..%zu", lo, hi, min_order, max_order);
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return fail(ZLFFT_ERR_CUDA, "no CUDA device");
+    DeviceGuard g(device);
+    const size_t es = prec == ZLFFT_F32 ? 4 : 8;
+    const size_t budget = size_t{512} << 20;
+    const size_t n_hi = size_t{1} << hi;
+    const size_t one = 2 * es * (n_hi + 2);  // largest single transform, either side
+    const size_t bytes = std::max(budget, one) + 256;
+    void* d_in = nullptr;
+    void* d_out = nullptr;
+    if (cudaMalloc(&d_in, bytes) != cudaSuccess || cudaMalloc(&d_out, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        if (d_in) cudaFree(d_in);
+        return fail(ZLFFT_ERR_ALLOC, "autotune buffers of %zu bytes failed", bytes);
+    }
+    cudaStream_t st = nullptr;
+    int rc = ZLFFT_OK;
+    cudaError_t e = cudaMemset(d_in, 0x3c, bytes);  // every float about 0.0115
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) rc = cuda_fail(e, "autotune set-up");
+    for (size_t order = lo; order <= hi && !rc; ++order) {
+        const size_t n = size_t{1} << order;
+        const int cfft_order = kind == ZLFFT_C2C ? (int)order : (int)order - 1;
+        const size_t per_in = kind == ZLFFT_C2C ? 2 * es * n : es * n;
+        const size_t per_out = kind == ZLFFT_C2C ? 2 * es * n : 2 * es * (n / 2 + 1);
+        const size_t batch = std::max<size_t>(1, budget / std::max(per_in, per_out));
+        std::vector<TuneEntry> cands;
+        const bool tc_ok = kind == ZLFFT_C2C && prec == ZLFFT_F32 && cfft_order >= zlfft::kPassMinP;
+        if (cfft_order >= zlfft::kPassMinP) {
+            for (int form : {ZLFFT_MODE_PLAIN, ZLFFT_MODE_TC_FP16}) {
+                if (form == ZLFFT_MODE_TC_FP16 && !tc_ok) continue;
+                for (int chunk : {16, 32, 48, 96, 192})
+                    for (int streams : {1, 2})
+                        for (int tma : {0, 1}) {
+                            TuneEntry c;
+                            c.chunk_mb = chunk;
+                            c.streams = streams;
+                            c.tma = tma;
+                            c.form = form;
+                            cands.push_back(c);
+                        }
+            }
+        } else {
+            for (int tma : {1, 0}) {
+                TuneEntry c;
+                c.chunk_mb = 0;
+                c.streams = 1;
+                c.tma = tma;
+                cands.push_back(c);
+            }
+        }
+        TuneEntry best;
+        double best_gbs = -1, def_gbs = 0;
+        for (const TuneEntry& c : cands) {
+            double ms = 0;
+            rc = time_candidate(device, kind, prec, (int)order, c, d_in, d_out, batch, st, &ms);
+            if (rc) break;
+            const double gbs = (double)batch * (double)(per_in + per_out) / (ms * 1e6);
+            const bool is_default = c.form == ZLFFT_MODE_PLAIN && c.tma == 1 &&
+                                    (c.chunk_mb == 0 || (c.chunk_mb == 48 && c.streams == 2));
+            if (is_default) def_gbs = gbs;
+            if (gbs > best_gbs) {
+                best_gbs = gbs;
+                best = c;
+            }
+        }
+        if (rc) break;
+        best.gbs = best_gbs;
+        best.gbs_default = def_gbs;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune[std::make_tuple(device, kind, prec, (int)order)] = best;
+    }
+    if (st) cudaStreamDestroy(st);
+    cudaFree(d_in);
+    cudaFree(d_out);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zlfft_autotune(int device, int kind, int precision, size_t order_lo, size_t order_hi) {
+    return autotune_impl(device, kind, precision, order_lo, order_hi);
+}
+
+int zlfft_tuning_get(int device, int kind, int precision, size_t order, zlfft_tuning* out) {
+    if (!out) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return fail(ZLFFT_ERR_CUDA, "no CUDA device");
+    TuneEntry e;
+    if (order > 64 || !tune_lookup(device, kind, precision, (int)order, &e))
+        return fail(ZLFFT_ERR_UNSUPPORTED, "no tuning entry for this size");
+    out->chunk_mb = e.chunk_mb;
+    out->streams = e.streams;
+    out->tma = e.tma;
+    out->form = e.form;
+    out->gbs = e.gbs;
+    out->gbs_default = e.gbs_default;
+    return ZLFFT_OK;
+}
+
+int zlfft_tuning_save(int device, const char* path) {
+    if (!path) return fail(ZLFFT_ERR_INVALID_ARG, "null path");
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return fail(ZLFFT_ERR_CUDA, "no CUDA device");
+    std::string name;
+    int sms = 0;
+    int rc = gpu_identity(device, &name, &sms);
+    if (rc) return rc;
+    FILE* f = fopen(path, "w");
+    if (!f) return fail(ZLFFT_ERR_INVALID_ARG, "cannot write tuning file %s", path);
+    fprintf(f, "# zlfft tuning table: entry kind precision order chunk_mb streams tma form gbs gbs_default\n");
+    fprintf(f, "gpu %s sms %d\n", name.c_str(), sms);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        for (const auto& kv : g_tune) {
+            if (std::get<0>(kv.first) != device) continue;
+            const TuneEntry& e = kv.second;
+            fprintf(f, "entry %d %d %d %d %d %d %d %.1f %.1f\n", std::get<1>(kv.first), std::get<2>(kv.first),
+                    std::get<3>(kv.first), e.chunk_mb, e.streams, e.tma, e.form, e.gbs, e.gbs_default);
+        }
+    }
+    if (fclose(f) != 0) return fail(ZLFFT_ERR_INVALID_ARG, "writing %s failed", path);
+    return ZLFFT_OK;
+}
+
+int zlfft_tuning_load(int device, const char* path, size_t* loaded) {
+    if (!path) return fail(ZLFFT_ERR_INVALID_ARG, "null path");
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return fail(ZLFFT_ERR_CUDA, "no CUDA device");
+    return tuning_load_impl(device, path, loaded);
+}
+
+int zlfft_tuning_clear(void) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune.clear();
+    return ZLFFT_OK;
+}
 
 }  // extern "C"

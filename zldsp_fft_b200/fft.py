@@ -252,3 +252,34 @@ class MixedBatch:
             self.close()
         except Exception:
             pass
+
+
+def autotune(kind: int, order_lo: int, order_hi: int, dtype=np.float32, device: int = -1) -> None:
+    """Measure the candidate plans of every order in [order_lo, order_hi] on the
+    device and record the fastest (zlfft_autotune); later plans use them."""
+    C.check(C.lib().zlfft_autotune(device, kind, _prec(dtype), int(order_lo), int(order_hi)))
+
+
+def tuning(kind: int, order: int, dtype=np.float32, device: int = -1):
+    """The tuning entry of a size as a dict, or None if it has none."""
+    t = C.Tuning()
+    rc = C.lib().zlfft_tuning_get(device, kind, _prec(dtype), int(order), ctypes.byref(t))
+    if rc == C.ERR_UNSUPPORTED:
+        return None
+    C.check(rc)
+    return {"chunk_mb": t.chunk_mb, "streams": t.streams, "tma": t.tma,
+            "form": "tc_fp16" if t.form == C.MODE_TC_FP16 else "plain", "gbs": t.gbs, "gbs_default": t.gbs_default}
+
+
+def tuning_save(path: str, device: int = -1) -> None:
+    C.check(C.lib().zlfft_tuning_save(device, path.encode()))
+
+
+def tuning_load(path: str, device: int = -1) -> int:
+    n = ctypes.c_size_t()
+    C.check(C.lib().zlfft_tuning_load(device, path.encode(), ctypes.byref(n)))
+    return n.value
+
+
+def tuning_clear() -> None:
+    C.check(C.lib().zlfft_tuning_clear())
