@@ -47,6 +47,7 @@ def test_autotune_records_entries_and_keeps_results(oracle):
     xr = rng.uniform(-1, 1, (8, 1 << 15)).astype(np.float32)
     p = Z.Plan(Z.R2C, 15, np.float32, mode=Z.MODE_TUNED)
     assert np.array_equal(G.run_r2c(p, xr), oracle.rfft_forward_port(xr))
+    assert Z.tuning(Z.R2C, 15, np.float32)["split_fused"] in (0, 1)
 
 
 def test_tuning_file_round_trip(tmp_path):
@@ -59,7 +60,7 @@ def test_tuning_file_round_trip(tmp_path):
     assert Z.tuning_load(path) == 2
     for o in (13, 14):
         got = Z.tuning(Z.C2C, o, np.float32)
-        for k in ("chunk_mb", "streams", "tma", "form"):
+        for k in ("chunk_mb", "streams", "tma", "form", "split_fused"):
             assert got[k] == want[o][k], (o, k)
     # a file written on another GPU model is not applied here
     other = tmp_path / "other.txt"
@@ -68,3 +69,47 @@ def test_tuning_file_round_trip(tmp_path):
     Z.tuning_clear()
     assert Z.tuning_load(str(other)) == 0
     assert Z.tuning(Z.C2C, 14, np.float32) is None
+
+
+def _this_gpu():
+    import torch
+    prop = torch.cuda.get_device_properties(0)
+    return prop.name.replace(" ", "_").replace("\t", "_"), prop.multi_processor_count
+
+
+@pytest.mark.parametrize("prec,dt", [("f32", np.float32), ("f64", np.float64)])
+def test_rfft_split_fused_into_last_pass(oracle, tmp_path, prec, dt):
+    """A tuning file can select the RFFT forward whose split runs inside the
+    last multi-pass pass (units paired with their mirrors in one CTA): same
+    bits as the oracle in FP32 (AoS, SoA, squared magnitudes), within the bar
+    in FP64, including batches of several chunks."""
+    name, sms = _this_gpu()
+    pv = 0 if dt == np.float32 else 1
+    lines = [f"gpu {name} sms {sms}"] + [f"entry 1 {pv} {o} 48 2 1 0 1 0 0" for o in (15, 16, 17)]
+    path = tmp_path / "fused.txt"
+    path.write_text("\n".join(lines) + "\n")
+    assert Z.tuning_load(str(path)) == 3
+    rng = np.random.default_rng(77)
+    for order, batch in ((15, 3), (16, 2), (17, 1)):
+        assert Z.tuning(Z.R2C, order, dt)["split_fused"] == 1
+        n = 1 << order
+        x = rng.uniform(-1, 1, (batch, n)).astype(dt)
+        plan = Z.Plan(Z.R2C, order, dt)
+        tol = oracle.tolerance(order, prec)
+        for ol in (Z.AOS, Z.SOA):
+            X = G.run_r2c(plan, x, ol)
+            assert oracle.rel_l2(X, oracle.rfft_fp64(x)).max() <= tol, (order, ol)
+            if prec == "f32":
+                assert np.array_equal(X, oracle.rfft_forward_port(x)), (order, ol)
+        P = G.run_r2c(plan, x, sqr_mag=True)
+        if prec == "f32":
+            assert np.array_equal(P, oracle.rfft_forward_port(x, sqr_mag=True)), order
+        else:
+            ref = np.abs(oracle.rfft_fp64(x)) ** 2
+            assert oracle.rel_l2(P, ref).max() <= 2 * tol
+    # 300 frames of order 16 at a 16 MiB chunk: many chunks on both pipelines
+    path.write_text(f"gpu {name} sms {sms}\nentry 1 {pv} 16 16 2 1 0 1 0 0\n")
+    assert Z.tuning_load(str(path)) == 1
+    x = rng.uniform(-1, 1, (300, 1 << 16)).astype(dt)
+    X = G.run_r2c(Z.Plan(Z.R2C, 16, dt), x, Z.AOS)
+    assert oracle.rel_l2(X, oracle.rfft_fp64(x)).max() <= oracle.tolerance(16, prec)

@@ -168,7 +168,7 @@ const TablesHolder& tables() {
 // Process-wide: (device, kind, precision, order) -> the plan parameters that
 // measured fastest there (zlfft_autotune), or that a tuning file recorded.
 struct TuneEntry {
-    int chunk_mb = 48, streams = 2, tma = 1, form = ZLFFT_MODE_PLAIN;
+    int chunk_mb = 48, streams = 2, tma = 1, form = ZLFFT_MODE_PLAIN, split_fused = 0;
     double gbs = 0, gbs_default = 0;
 };
 std::mutex g_tune_mu;
@@ -217,15 +217,15 @@ int tuning_load_impl(int device, const char* path, size_t* loaded) {
             same_gpu = (name == gname && sms == gsms);
             continue;
         }
-        int kind, prec, order, chunk, streams, tma, form;
+        int kind, prec, order, chunk, streams, tma, form, fused;
         double gbs, gbs0;
-        if (sscanf(line, "entry %d %d %d %d %d %d %d %lf %lf", &kind, &prec, &order, &chunk, &streams, &tma, &form,
-                   &gbs, &gbs0) != 9)
+        if (sscanf(line, "entry %d %d %d %d %d %d %d %d %lf %lf", &kind, &prec, &order, &chunk, &streams, &tma, &form,
+                   &fused, &gbs, &gbs0) != 10)
             continue;
         if (!same_gpu) continue;
         const bool ok = (kind == ZLFFT_C2C || kind == ZLFFT_R2C) && (prec == ZLFFT_F32 || prec == ZLFFT_F64) &&
                         order >= 0 && order <= zlfft::kPassMaxP + 1 && chunk >= 0 && chunk <= 4096 &&
-                        (streams == 1 || streams == 2) && (tma == 0 || tma == 1) &&
+                        (streams == 1 || streams == 2) && (tma == 0 || tma == 1) && (fused == 0 || fused == 1) &&
                         (form == ZLFFT_MODE_PLAIN ||
                          (form == ZLFFT_MODE_TC_FP16 && kind == ZLFFT_C2C && prec == ZLFFT_F32));
         if (!ok) continue;
@@ -234,6 +234,7 @@ int tuning_load_impl(int device, const char* path, size_t* loaded) {
         e.streams = streams;
         e.tma = tma;
         e.form = form;
+        e.split_fused = fused;
         e.gbs = gbs;
         e.gbs_default = gbs0;
         std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -282,6 +283,7 @@ struct zlfft_plan_s {
     int nlanes = 2;         // chunk pipelines
     int use_tma = 1;        // TMA staging of kernel inputs (else direct loads)
     bool tc_form = false;   // 256-point passes in the tensor-core split form
+    bool fuse_split = false;  // RFFT forward: split fused into the last pass (else its own kernel)
     std::mutex mu;
 };
 
@@ -506,6 +508,7 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
             src_layout = ZLFFT_AOS;
         }
         char* bufs[2] = {c2r ? s1 : s0, c2r ? s0 : s1};
+        bool split_done = false;
         for (int pi = 0; pi < np; ++pi) {
             const bool last = (pi + 1 == np);
             const bool gfirst = gather && pi == 0 && !c2r;  // the first pass reads gathered inputs
@@ -528,12 +531,19 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
                 pa.tma = (p->use_tma && !gfirst && aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
                           (nb == 1 || ((size_t)src_stride * eb) % 16 == 0)) ? 1 : 0;
             }
-            if (last && !r2c) {
+            // RFFT forward: the last pass fuses the split and writes the bins
+            zlfft::PassLaunchFn split_fn = nullptr;
+            if (p->fuse_split && last && r2c && !p->tc_form) {
+                const zlfft::PassTable& tt = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
+                split_fn = tt.split[P - zlfft::kPassMinP][dop == zlfft::kR2CSqrMag ? 1 : 0][out_layout];
+            }
+            if ((last && !r2c) || split_fn) {
                 pa.out0 = uo0;
                 pa.out1 = uo1;
                 pa.out_stride = a.out_stride;
                 pa.gout0 = go0;
                 pa.gout1 = go1;
+                pa.rw = p->d_rw;
             } else {
                 pa.out0 = bufs[pi & 1];
                 pa.out1 = nullptr;
@@ -541,15 +551,16 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
             }
             const int li = pi == 0 ? src_layout : ZLFFT_AOS;
             const int lo = (last && !r2c) ? ol : ZLFFT_AOS;
-            zlfft::PassLaunchFn fn = pick_pass(p, pi, fwd, li, lo);
+            zlfft::PassLaunchFn fn = split_fn ? split_fn : pick_pass(p, pi, fwd, li, lo);
             if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no pass kernel for order %d", p->order);
             e = fn(pa, st, ctx);
             if (e != cudaSuccess) return cuda_fail(e, "pass launch");
             src0 = pa.out0;
             src1 = nullptr;
             src_stride = n;
+            if (split_fn) split_done = true;
         }
-        if (r2c) {
+        if (r2c && !split_done) {
             e = p->prec == ZLFFT_F32
                     ? launch_split<float>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx, go0, go1)
                     : launch_split<double>(p, dop, out_layout, src0, uo0, uo1, nb, a.out_stride, st, ctx, go0, go1);
@@ -1274,6 +1285,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
             if (te.chunk_mb > 0) p->chunk_mb = (size_t)te.chunk_mb;
             p->nlanes = te.streams;
             p->use_tma = te.tma;
+            p->fuse_split = te.split_fused != 0;
             if (mode == ZLFFT_MODE_TUNED && te.form == ZLFFT_MODE_TC_FP16) p->tc_form = true;
         }
         if (mode == ZLFFT_MODE_TC_FP16) p->tc_form = true;
@@ -1562,6 +1574,7 @@ int time_candidate(int device, int kind, int prec, int order, const TuneEntry& c
     p->chunk_mb = c.chunk_mb > 0 ? (size_t)c.chunk_mb : p->chunk_mb;
     p->nlanes = c.streams;
     p->use_tma = c.tma;
+    p->fuse_split = c.split_fused != 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1628,14 +1641,17 @@ int autotune_impl(int device, int kind, int prec, size_t lo, size_t hi) {
                 if (form == ZLFFT_MODE_TC_FP16 && !tc_ok) continue;
                 for (int chunk : {16, 32, 48, 96, 192})
                     for (int streams : {1, 2})
-                        for (int tma : {0, 1}) {
-                            TuneEntry c;
-                            c.chunk_mb = chunk;
-                            c.streams = streams;
-                            c.tma = tma;
-                            c.form = form;
-                            cands.push_back(c);
-                        }
+                        for (int tma : {0, 1})
+                            for (int fused : {0, 1}) {
+                                if (fused && kind != ZLFFT_R2C) continue;
+                                TuneEntry c;
+                                c.chunk_mb = chunk;
+                                c.streams = streams;
+                                c.tma = tma;
+                                c.form = form;
+                                c.split_fused = fused;
+                                cands.push_back(c);
+                            }
             }
         } else {
             for (int tma : {1, 0}) {
@@ -1653,7 +1669,7 @@ int autotune_impl(int device, int kind, int prec, size_t lo, size_t hi) {
             rc = time_candidate(device, kind, prec, (int)order, c, d_in, d_out, batch, st, &ms);
             if (rc) break;
             const double gbs = (double)batch * (double)(per_in + per_out) / (ms * 1e6);
-            const bool is_default = c.form == ZLFFT_MODE_PLAIN && c.tma == 1 &&
+            const bool is_default = c.form == ZLFFT_MODE_PLAIN && c.tma == 1 && c.split_fused == 0 &&
                                     (c.chunk_mb == 0 || (c.chunk_mb == 48 && c.streams == 2));
             if (is_default) def_gbs = gbs;
             if (gbs > best_gbs) {
@@ -1691,6 +1707,7 @@ int zlfft_tuning_get(int device, int kind, int precision, size_t order, zlfft_tu
     out->streams = e.streams;
     out->tma = e.tma;
     out->form = e.form;
+    out->split_fused = e.split_fused;
     out->gbs = e.gbs;
     out->gbs_default = e.gbs_default;
     return ZLFFT_OK;
@@ -1705,15 +1722,16 @@ int zlfft_tuning_save(int device, const char* path) {
     if (rc) return rc;
     FILE* f = fopen(path, "w");
     if (!f) return fail(ZLFFT_ERR_INVALID_ARG, "cannot write tuning file %s", path);
-    fprintf(f, "# zlfft tuning table: entry kind precision order chunk_mb streams tma form gbs gbs_default\n");
+    fprintf(f, "# zlfft tuning table: entry kind precision order chunk_mb streams tma form split_fused gbs "
+               "gbs_default\n");
     fprintf(f, "gpu %s sms %d\n", name.c_str(), sms);
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         for (const auto& kv : g_tune) {
             if (std::get<0>(kv.first) != device) continue;
             const TuneEntry& e = kv.second;
-            fprintf(f, "entry %d %d %d %d %d %d %d %.1f %.1f\n", std::get<1>(kv.first), std::get<2>(kv.first),
-                    std::get<3>(kv.first), e.chunk_mb, e.streams, e.tma, e.form, e.gbs, e.gbs_default);
+            fprintf(f, "entry %d %d %d %d %d %d %d %d %.1f %.1f\n", std::get<1>(kv.first), std::get<2>(kv.first),
+                    std::get<3>(kv.first), e.chunk_mb, e.streams, e.tma, e.form, e.split_fused, e.gbs, e.gbs_default);
         }
     }
     if (fclose(f) != 0) return fail(ZLFFT_ERR_INVALID_ARG, "writing %s failed", path);

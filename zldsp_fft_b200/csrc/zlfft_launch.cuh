@@ -103,6 +103,9 @@ struct PassTable {
     // [order - kPassMinP][pass][fwd][in_layout][out_layout]; the layouts only
     // matter on the first (input) and last (output) pass.
     PassLaunchFn fn[kPassMaxP - kPassMinP + 1][kMaxPasses][2][2][2];
+    // [order - kPassMinP][0: RFFT forward, 1: forward_sqr_mag][output layout]: the
+    // last pass with the RFFT split fused (the N/2-point spectrum never leaves the CTA)
+    PassLaunchFn split[kPassMaxP - kPassMinP + 1][2][2];
 };
 
 // cuTensorMapEncodeTiled, reached through the runtime's driver entry point
@@ -150,10 +153,10 @@ bool encode_pass_maps(const PassArgs& a, PassMaps& m) {
     return true;
 }
 
-template <typename F, int P, int PI, bool FWD, int IL, int OL>
+template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0>
 cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = PassCfg<F, P, PI>;
-    auto kern = pass_kernel<F, P, PI, FWD, IL, OL>;
+    auto kern = pass_kernel<F, P, PI, FWD, IL, OL, SPLIT>;
     constexpr int IL2 = Cfg::FIRST ? IL : (int)kAoS;
     PassArgs a = a_in;
     PassMaps maps;
@@ -163,7 +166,10 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
         const char* e = getenv("ZLFFT_PASS_TMA");
         return !(e && e[0] == '0');
     }();
-    a.tma = (tma_enabled && a.tma && !(Cfg::FIRST && a.gin0) && encode_pass_maps<F, P, PI, IL2>(a, maps)) ? 1 : 0;
+    // (the split-fused last pass reads mirror-paired units directly)
+    a.tma = (SPLIT == 0 && tma_enabled && a.tma && !(Cfg::FIRST && a.gin0) && encode_pass_maps<F, P, PI, IL2>(a, maps))
+                ? 1
+                : 0;
     static const int blocks_per_sm = [kern]() {
         if (Cfg::SMEM > 48 * 1024)
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
@@ -220,6 +226,12 @@ void fill_pass_order(PassTable& t) {
     fill_pass_one<F, P, 0>(t);
     fill_pass_one<F, P, 1>(t);
     if constexpr (pass_count(P) > 2) fill_pass_one<F, P, 2>(t);
+    // last pass with the RFFT split fused: [forward | sqr_mag][output layout]
+    constexpr int PL = pass_count(P) - 1;
+    auto& sp = t.split[P - kPassMinP];
+    sp[0][kAoS] = launch_pass<F, P, PL, true, kAoS, kAoS, kR2CFwd>;
+    sp[0][kSoA] = launch_pass<F, P, PL, true, kAoS, kSoA, kR2CFwd>;
+    sp[1][kAoS] = sp[1][kSoA] = launch_pass<F, P, PL, true, kAoS, kAoS, kR2CSqrMag>;
 }
 
 template <typename F, int... Ps>

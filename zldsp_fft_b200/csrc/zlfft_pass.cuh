@@ -106,6 +106,7 @@ struct PassArgs {
     const void* tws;       // per-stage twiddle tables (stage_l0 layout)
     const void* tw;        // unified table T[t] = W_N^t, t < 3N/4 (tensor-core passes)
     const void* tctw;      // this pass's tensor-core twiddles when L_in > 1 (zlfft_tc_pass.cuh)
+    const void* rw;        // RFFT split twiddle pairs (last pass with the split fused)
     int* err;              // device error word (kDevErrWaitTimeout on a timed-out wait)
     int tma;               // the tensor maps describe the input (else direct loads)
     // Gathered transforms (mixed batches): the first pass reads transform t
@@ -124,10 +125,31 @@ struct PassMaps {
     CUtensorMap m1;
 };
 
+// Unit of slot u in work item ib of a last pass with the RFFT split fused:
+// the first half of the slots take units HALF*ib + u, the second half their
+// mirrors L_in - (HALF*ib + u) (unit L_in/2 stands in for the mirror of unit
+// 0), so every Z[k] of the item meets Z[M - k] in the same CTA: position
+// p = k + pos * L_in of a low unit k >= 1 mirrors to unit L_in - k at
+// position R - 1 - pos.
+template <int L_IN, int UPC>
+__device__ __forceinline__ int split_unit(int ib, int u) {
+    constexpr int HALF = UPC / 2;
+    if (u < HALF) return HALF * ib + u;
+    const int v = HALF * ib + (u - HALF);
+    return v == 0 ? L_IN / 2 : L_IN - v;
+}
+
 // One pass over `batch` transforms. FWD selects the direction swap on the
 // first pass's loads and the last pass's stores (the reference's backward
 // transform is swap(DFT(swap(x))), src/common/zldsp_fft_common_structure.hpp:47-95).
-template <typename F, int P, int PI, bool FWD, int IL, int OL>
+//
+// SPLIT (kR2CFwd or kR2CSqrMag, last pass of an RFFT forward only) fuses the
+// RFFT split: the item's spectrum values go to shared memory in [pos][slot]
+// order, the slots hold mirror pairs of units (split_unit), and the epilogue
+// writes bins k and M - k of every pair with the reference's arithmetic
+// (src/common/zldsp_fft_common_execute.hpp:318-368, :481-536), as
+// rfft_split_kernel does.
+template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0>
 __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>::MINB)
     pass_kernel(const PassArgs a, const __grid_constant__ PassMaps maps) {
     using Cfg = PassCfg<F, P, PI>;
@@ -149,7 +171,8 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
     constexpr int CMP = kSoAIn ? 1 : 2;  // scalars per unit in the map's innermost dimension
     C* stage = reinterpret_cast<C*>(smem_raw + Cfg::SOFF);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::SOFF + Cfg::SBYTES);
-    const bool use_tma = Cfg::kTMA && a.tma;
+    static_assert(SPLIT == 0 || (Cfg::LAST && FWD && L_IN > 1 && Cfg::UPC >= 2), "split fusion: RFFT forward last pass");
+    const bool use_tma = Cfg::kTMA && a.tma && SPLIT == 0;
     auto issue = [&](long long it) {  // one thread issues the item's box copies
         if (!use_tma || threadIdx.x != 0 || it >= items) return;
         const int z = (int)(it / Cfg::CPT);
@@ -180,7 +203,8 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
 
     for (long long item = blockIdx.x; item < items; item += gridDim.x) {
         const long long tr = item / Cfg::CPT;
-        const int U = (int)(item % Cfg::CPT) * UPC + u;
+        const int ib = (int)(item % Cfg::CPT);
+        const int U = SPLIT ? split_unit<L_IN, UPC>(ib, u) : ib * UPC + u;
         const int ku = U % L_IN;  // k of the unit
         const int J = U / L_IN;
         C v[E];
@@ -286,6 +310,15 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                             out.put(e, (Cfg::LAST && !FWD) ? cswap(x) : x);
                         }
                         __syncthreads();
+                    } else if constexpr (SPLIT != 0) {
+                        // spectrum values of the item to shared memory, [pos][slot]
+                        __syncthreads();
+#pragma unroll
+                        for (int i = 0; i < NB; ++i) {
+                            const int b = tb + i * T;
+#pragma unroll
+                            for (int s = 0; s < G.R; ++s) sm[(b + group_mu(G, s) * ELL) * ROW + u] = v[i * G.R + s];
+                        }
                     } else {
                         const bool g = Cfg::LAST && a.gout0 != nullptr;
                         const CxOut<F, OL2> out(g ? a.gout0[tr] : a.out0, g ? (a.gout1 ? a.gout1[tr] : nullptr) : a.out1,
@@ -304,6 +337,69 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                 }(),
                 ...);
         }(std::make_integer_sequence<int, GE - GB>{});
+        if constexpr (SPLIT != 0) {
+            // ---- fused RFFT split over the item's mirror pairs (M = N complex points)
+            __syncthreads();
+            constexpr int HALF = UPC / 2;
+            const bool first_item = (ib == 0);
+            const int tasks = HALF * R + (first_item ? 1 : 0);
+            const C* rw = static_cast<const C*>(a.rw);
+            const bool g = a.gout0 != nullptr;
+            void* o0 = g ? a.gout0[tr] : a.out0;
+            void* o1 = g ? (a.gout1 ? a.gout1[tr] : nullptr) : a.out1;
+            const long long ob = g ? 0 : tr * a.out_stride;
+            constexpr int OLS = (SPLIT == kR2CSqrMag) ? (int)kAoS : OL;
+            const CxOut<F, OLS> out(o0, o1, ob);
+            F* osq = static_cast<F*>(o0) + ob;
+            for (int t = (int)threadIdx.x; t < tasks; t += Cfg::THREADS) {
+                const int pos = t / HALF, us = t % HALF;
+                int s1, p1, s2, p2;  // slot and position of the pair's two values
+                if (first_item && us == 0) {
+                    if (pos <= R / 2) {  // unit 0 pairs with itself
+                        s1 = 0;
+                        p1 = pos;
+                        s2 = 0;
+                        p2 = (R - pos) & (R - 1);
+                    } else {  // unit L_in/2 pairs with itself
+                        const int ph = pos - R / 2 - 1;
+                        s1 = HALF;
+                        p1 = ph;
+                        s2 = HALF;
+                        p2 = R - 1 - ph;
+                    }
+                } else {
+                    s1 = us;
+                    p1 = pos;
+                    s2 = us + HALF;
+                    p2 = R - 1 - pos;
+                }
+                const int g1 = split_unit<L_IN, UPC>(ib, s1) + p1 * L_IN;
+                if (g1 == 0) {  // DC and Nyquist from Z[0]
+                    const C z0 = sm[p1 * ROW + s1];
+                    const F dc = z0.x + z0.y, ny = z0.x - z0.y;
+                    if constexpr (SPLIT == kR2CFwd) {
+                        out.put(0, cx<C>(dc, (F)0));
+                        out.put(N, cx<C>(ny, (F)0));
+                    } else {
+                        osq[0] = mul_rn(dc, dc);
+                        osq[N] = mul_rn(ny, ny);
+                    }
+                    continue;
+                }
+                const C za = sm[p1 * ROW + s1], zb = sm[p2 * ROW + s2];
+                const bool low = g1 <= N / 2;  // k = min(g1, N - g1)
+                const int k = low ? g1 : N - g1;
+                const C w = rw[k];
+                const SplitOut<F> o = rfft_split<F>(low ? za : zb, low ? zb : za, w.x, w.y);
+                if constexpr (SPLIT == kR2CFwd) {
+                    if (k != N / 2) out.put(k, cx<C>(o.xr_k, o.xi_k));
+                    out.put(N - k, cx<C>(o.xr_m, o.xi_m));
+                } else {
+                    if (k != N / 2) osq[k] = fma_rn(o.xr_k, o.xr_k, mul_rn(o.xi_k, o.xi_k));
+                    osq[N - k] = fma_rn(o.xr_m, o.xr_m, mul_rn(o.xi_m, o.xi_m));
+                }
+            }
+        }
         // shared memory is rewritten by the next item's first exchange only after a barrier
     }
 }

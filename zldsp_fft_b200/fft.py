@@ -268,7 +268,8 @@ def tuning(kind: int, order: int, dtype=np.float32, device: int = -1):
         return None
     C.check(rc)
     return {"chunk_mb": t.chunk_mb, "streams": t.streams, "tma": t.tma,
-            "form": "tc_fp16" if t.form == C.MODE_TC_FP16 else "plain", "gbs": t.gbs, "gbs_default": t.gbs_default}
+            "form": "tc_fp16" if t.form == C.MODE_TC_FP16 else "plain", "split_fused": t.split_fused,
+            "gbs": t.gbs, "gbs_default": t.gbs_default}
 
 
 def tuning_save(path: str, device: int = -1) -> None:
