@@ -419,7 +419,8 @@ class Mixed:
     count = 20000
     dtype = "f32"
 
-    def __init__(self):
+    def __init__(self, autotune=True):
+        self.autotune = autotune
         rng = np.random.default_rng(1004)
         self.orders = rng.integers(6, 17, self.count)
         self.is_c = rng.random(self.count) < 0.5
@@ -448,8 +449,9 @@ class Mixed:
         a, b = self.A.data_ptr(), self.B.data_ptr()
         # autotuned plan per order (set-up, outside the timed region): the batch's
         # plans are created in the tuned mode
-        Z.autotune(Z.C2C, 6, 16, np.float32, device=device)
-        Z.autotune(Z.R2C, 6, 16, np.float32, device=device)
+        if self.autotune:
+            Z.autotune(Z.C2C, 6, 16, np.float32, device=device)
+            Z.autotune(Z.R2C, 6, 16, np.float32, device=device)
         self.tuning = {f"{'c2c' if k == Z.C2C else 'r2c'}{o}": Z.tuning(k, o, np.float32, device=device)
                        for k in (Z.C2C, Z.R2C) for o in range(14, 17)}
         descs = [(Z.C2C if c else Z.R2C, int(o), Z.FORWARD, a + int(io), b + int(oo))
@@ -719,21 +721,31 @@ class Cfft10:
             bwd(s.cuda_stream)
         torch.cuda.synchronize(device)
         self.graphs = {}
+        self.graph_kernels = {}  # kernels recorded in each graph (the plan's launch counter)
+        self.launches = 0
+        p.take_launch_count()
         for name, fn in (("c2c_fwd", fwd), ("c2c_bwd", bwd)):
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=s):
                 fn(s.cuda_stream)
             self.graphs[name] = g
+            self.graph_kernels[name] = p.take_launch_count()
         torch.cuda.synchronize(device)
 
     def flush(self, st):
         self.flush_buf.fill_(1.0)
 
+    def _replay(self, name):
+        self.graphs[name].replay()
+        self.launches += self.graph_kernels[name]
+
     def ops(self, step):
-        return [(name, lambda st, g=g: g.replay()) for name, g in self.graphs.items()]
+        return [(name, lambda st, n=name: self._replay(n)) for name in self.graphs]
 
     def take_launches(self):
-        return self.plan.take_launch_count()
+        n = self.launches + self.plan.take_launch_count()
+        self.launches = 0
+        return n
 
     def compare(self, stream, reps):
         """Microseconds per transform and the error of forward (vs numpy FP64)
@@ -980,6 +992,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cfft2g")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="mixed only: skip the per-order autotuning in set-up (for profiling runs)")
     ap.add_argument("--form", choices=["plain", "tc"], default="plain",
                     help="cfft2g only: the plain FP32 form or the tensor-core split FP16 hi/lo form")
     ap.add_argument("--total-log2", type=int, default=None,
@@ -992,6 +1006,10 @@ def main():
         tl = args.total_log2 if args.total_log2 is not None else 28
         wl_cls = lambda: base(total_log2=tl, form=args.form)  # noqa: E731
         wl_cls.__name__ = base.__name__
+    if args.workload == "mixed" and args.no_autotune:
+        base_m = wl_cls
+        wl_cls = lambda: base_m(autotune=False)  # noqa: E731
+        wl_cls.__name__ = base_m.__name__
     if args.impl == "reference":
         return run_reference_arm(args, wl_cls)
     return run_ours(args, wl_cls)
