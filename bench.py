@@ -921,12 +921,9 @@ def run_ours(args, wl_cls):
         elapsed_ms = sum(ev[s][0].elapsed_time(ev[s][-1]) for s in range(args.steps))
     per_op_ms = {name: statistics.mean(ev[s][i].elapsed_time(ev[s][i + 1]) for s in range(args.steps))
                  for i, name in enumerate(names)}
-    if dist is not None:
-        t = torch.tensor([elapsed_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
-    total_bytes = wl.bytes_per_step * args.steps * world
-    value = total_bytes / (elapsed_ms / 1e3) / 1e9
+    from zldsp_fft_b200 import replicas
+    elapsed_ms = replicas.max_over_ranks(elapsed_ms, dist, device="cuda")
+    value = replicas.aggregate_gbs(wl.bytes_per_step * args.steps, world, elapsed_ms / 1e3)
 
     # end to end through the host API, pinned host buffers, copies inside the region
     wl.setup_e2e()
@@ -937,11 +934,8 @@ def run_ours(args, wl_cls):
     for _ in range(e2e_steps):
         wl.e2e_step()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_val = wl.bytes_per_step * e2e_steps * world / e2e_s / 1e9
+    e2e_s = replicas.max_over_ranks(e2e_s, dist, device="cuda")
+    e2e_val = replicas.aggregate_gbs(wl.bytes_per_step * e2e_steps, world, e2e_s)
     wl.take_launches()
     schedules = wl.compare(stream, max(3, min(args.steps, 10))) if hasattr(wl, "compare") else None
 
