@@ -119,6 +119,21 @@ ZLFFT_API int zlfft_exec_host_batched(zlfft_plan plan, int op, int in_layout, in
 ZLFFT_API int zlfft_exec_device(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0, const void* in1,
                       void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, void* stream);
 
+/* Short-time Fourier transform front end on DEVICE buffers: frame f of a
+ * real signal is signal[f*hop + n] * window[n], n < N (N = the RFFT plan's
+ * real length), and each frame goes through RFFT::forward (op FORWARD, bins
+ * in out_layout AoS or SoA) or RFFT::forward_sqr_mag (op FORWARD_SQR_MAG,
+ * N/2+1 reals) (src/zldsp_fft_rfft.hpp:68-80, :104-109), frame f's output at
+ * out + f*out_stride (0 = dense). One launch: frames are read straight from the
+ * signal and windowed as they are loaded; no framed copy is made. window NULL
+ * means a rectangular window. hop must be even; the signal must hold
+ * (n_frames - 1) * hop + N samples. Frame orders up to 14 (N <= 16384). No
+ * reference counterpart: a spectrum analyser built on the reference calls
+ * forward_sqr_mag frame by frame on copies it windows itself. */
+ZLFFT_API int zlfft_stft_device(zlfft_plan plan, int op, int out_layout, const void* signal, size_t hop,
+                                const void* window, void* out0, void* out1, size_t n_frames, size_t out_stride,
+                                void* stream);
+
 /* As zlfft_exec_device, for callers that cannot allocate device memory when
  * they run a transform: a real-time audio thread (an allocation can block
  * for an unbounded time), work being captured into a CUDA graph (cudaMalloc

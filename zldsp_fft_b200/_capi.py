@@ -52,6 +52,7 @@ EXPORTS = (
     "zlfft_exec_host_batched",
     "zlfft_exec_device",
     "zlfft_exec_device_noalloc",
+    "zlfft_stft_device",
     "zlfft_plan_take_launch_count",
     "zlfft_plan_copy_twiddles",
     "zlfft_plan_device_status",
@@ -104,6 +105,7 @@ def lib() -> ctypes.CDLL:
         L.zlfft_exec_host_batched.argtypes = [vp, i, i, i, vp, vp, vp, vp, sz]
         L.zlfft_exec_device.argtypes = [vp, i, i, i, vp, vp, vp, vp, sz, sz, sz, vp]
         L.zlfft_exec_device_noalloc.argtypes = [vp, i, i, i, vp, vp, vp, vp, sz, sz, sz, vp]
+        L.zlfft_stft_device.argtypes = [vp, i, i, vp, sz, vp, vp, vp, sz, sz, vp]
         L.zlfft_plan_take_launch_count.argtypes = [vp, ctypes.POINTER(sz)]
         L.zlfft_plan_copy_twiddles.argtypes = [vp, vp, sz, ctypes.POINTER(sz)]
         L.zlfft_plan_device_status.argtypes = [vp, ctypes.POINTER(i)]

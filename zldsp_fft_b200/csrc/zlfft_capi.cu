@@ -647,6 +647,57 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     return ZLFFT_OK;
 }
 
+// ------------------------------------------------------------------ STFT front end
+// Frames f = 0..n_frames-1 of a real signal, frame f = signal[f*hop + n] *
+// window[n] (n < N), each through the RFFT forward (bins or squared
+// magnitudes), in one launch of the tile kernel: the frames are read straight
+// from the signal (overlapping reads at stride hop) and windowed as they are
+// loaded, so no framed or windowed copy is ever written.
+int stft_impl(zlfft_plan_s* p, int op, int out_layout, const void* signal, size_t hop, const void* window,
+              void* out0, void* out1, size_t n_frames, size_t out_stride, cudaStream_t stream) {
+    if (p->kind != ZLFFT_R2C) return fail(ZLFFT_ERR_INVALID_ARG, "the STFT needs an RFFT plan");
+    if (op != ZLFFT_FORWARD && op != ZLFFT_FORWARD_SQR_MAG)
+        return fail(ZLFFT_ERR_INVALID_ARG, "STFT op must be FORWARD or FORWARD_SQR_MAG");
+    if (out_layout != ZLFFT_AOS && out_layout != ZLFFT_SOA) return fail(ZLFFT_ERR_INVALID_ARG, "invalid layout");
+    if (p->cfft_order > zlfft::kTileMaxP)
+        return fail(ZLFFT_ERR_UNSUPPORTED, "STFT frames up to order %d", zlfft::kTileMaxP + 1);
+    if (hop == 0 || hop % 2) return fail(ZLFFT_ERR_INVALID_ARG, "hop must be even and positive (frames are read as pairs)");
+    const bool soa = op == ZLFFT_FORWARD && out_layout == ZLFFT_SOA;
+    if (!signal || !out0 || (soa && !out1)) return fail(ZLFFT_ERR_INVALID_ARG, "null buffer pointer");
+    const size_t pair = 2 * p->esize;
+    if (!aligned(signal, pair) || (window && !aligned(window, pair)))
+        return fail(ZLFFT_ERR_ALIGNMENT, "signal and window must be %zu-byte aligned", pair);
+    if (!aligned(out0, op == ZLFFT_FORWARD && !soa ? pair : p->esize) || (soa && !aligned(out1, p->esize)))
+        return fail(ZLFFT_ERR_ALIGNMENT, "outputs must be aligned to their element type");
+    const size_t nb = (size_t{1} << p->order) / 2 + 1;
+    if (out_stride == 0) out_stride = nb;
+    if (n_frames > 1 && out_stride < nb) return fail(ZLFFT_ERR_INVALID_ARG, "output stride smaller than one frame");
+    if (n_frames == 0) return ZLFFT_OK;
+    zlfft::TileArgs a{};
+    a.in0 = signal;
+    a.out0 = out0;
+    a.out1 = soa ? out1 : nullptr;
+    a.batch = (long long)n_frames;
+    a.in_stride = (long long)(hop / 2);  // in complex pairs
+    a.out_stride = (long long)out_stride;
+    a.tw = p->d_tw;
+    a.tws = p->d_tws;
+    a.rw = p->d_rw;
+    a.err = p->d_err;
+    a.win = window;
+    a.tma = (p->use_tma && aligned(signal, 16) && (n_frames == 1 || (hop * p->esize) % 16 == 0)) ? 1 : 0;
+    const int dop = op == ZLFFT_FORWARD ? zlfft::kR2CFwd : zlfft::kR2CSqrMag;
+    const zlfft::TileTable& t = p->prec == ZLFFT_F32 ? tables().f32 : tables().f64;
+    zlfft::TileLaunchFn fn = window ? t.stft[p->cfft_order][op == ZLFFT_FORWARD ? 0 : 1][soa ? ZLFFT_SOA : ZLFFT_AOS]
+                                    : t.fn[p->cfft_order][dop][ZLFFT_AOS][soa ? ZLFFT_SOA : ZLFFT_AOS];
+    if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no kernel for this configuration");
+    zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
+    DeviceGuard g(p->device);
+    cudaError_t e = fn(a, stream, ctx);
+    if (e != cudaSuccess) return cuda_fail(e, "STFT launch");
+    return ZLFFT_OK;
+}
+
 // ------------------------------------------------------------------ allocation-free execution
 // Some callers cannot allocate device memory at the moment they run a
 // transform: a real-time audio callback must not block on the allocator,
@@ -1423,6 +1474,13 @@ int zlfft_exec_device(zlfft_plan plan, int op, int in_layout, int out_layout, co
     if (!plan) return fail(ZLFFT_ERR_INVALID_ARG, "null plan");
     return exec_device_impl(plan, op, in_layout, out_layout, in0, in1, out0, out1, batch, in_stride, out_stride,
                             static_cast<cudaStream_t>(stream));
+}
+
+int zlfft_stft_device(zlfft_plan plan, int op, int out_layout, const void* signal, size_t hop, const void* window,
+                      void* out0, void* out1, size_t n_frames, size_t out_stride, void* stream) {
+    if (!plan) return fail(ZLFFT_ERR_INVALID_ARG, "null plan");
+    return stft_impl(plan, op, out_layout, signal, hop, window, out0, out1, n_frames, out_stride,
+                     static_cast<cudaStream_t>(stream));
 }
 
 int zlfft_exec_device_noalloc(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0,

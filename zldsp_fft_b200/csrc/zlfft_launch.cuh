@@ -30,12 +30,15 @@ using TileLaunchFn = cudaError_t (*)(const TileArgs&, cudaStream_t, const Launch
 struct TileTable {
     // [order][op][in_layout][out_layout]
     TileLaunchFn fn[kTileMaxP + 1][5][2][2];
+    // STFT front end: RFFT forward with the window multiplied in at load,
+    // [order][0: forward, 1: forward_sqr_mag][out_layout]
+    TileLaunchFn stft[kTileMaxP + 1][2][2];
 };
 
-template <typename F, int P, int OP, int IL, int OL>
+template <typename F, int P, int OP, int IL, int OL, bool WIN = false>
 cudaError_t launch_tile(const TileArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = TileCfg<F, P, OP>;
-    auto kern = tile_kernel<F, P, OP, IL, OL>;
+    auto kern = tile_kernel<F, P, OP, IL, OL, false, WIN>;
     static const int blocks_per_sm = [kern]() {
         if (Cfg::SMEM > 48 * 1024) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
@@ -362,6 +365,9 @@ void fill_tile_r2c_order(TileTable& t) {
         t.fn[P][kC2RBwd][kAoS][ol] = launch_tile<F, P, kC2RBwd, kAoS, kAoS>;
         t.fn[P][kC2RBwd][kSoA][ol] = launch_tile<F, P, kC2RBwd, kSoA, kAoS>;
     }
+    t.stft[P][0][kAoS] = launch_tile<F, P, kR2CFwd, kAoS, kAoS, true>;
+    t.stft[P][0][kSoA] = launch_tile<F, P, kR2CFwd, kAoS, kSoA, true>;
+    t.stft[P][1][kAoS] = t.stft[P][1][kSoA] = launch_tile<F, P, kR2CSqrMag, kAoS, kAoS, true>;
 }
 
 template <typename F, int... Ps>

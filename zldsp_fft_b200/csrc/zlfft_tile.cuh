@@ -127,6 +127,9 @@ struct TileArgs {
     const void* const* gin1;
     void* const* gout0;
     void* const* gout1;
+    // RFFT forward only: window multiplied into every frame as it is loaded
+    // (the STFT front end); pairs (w[2i], w[2i+1]) per complex-pair input.
+    const void* win;
 };
 
 template <typename F, int P, int OP = kC2CFwd, int BLOCK = 128>
@@ -372,7 +375,7 @@ __device__ __forceinline__ SplitOut<F> rfft_split(C z1, C z2, F c, F s) {
 // and the processing of one tile. tile_kernel drives it over a contiguous
 // batch with TMA prefetch; mixed_kernel (zlfft_mixed.cuh) drives it over a
 // queue of tiles of many orders.
-template <typename F, int P, int OP, int IL, int OL, int BLOCK = 128, bool GATHER = false>
+template <typename F, int P, int OP, int IL, int OL, int BLOCK = 128, bool GATHER = false, bool WIN = false>
 struct TileWorker {
     using Cfg = TileCfg<F, P, OP, BLOCK>;
     using C = Cx<F>;
@@ -473,6 +476,12 @@ struct TileWorker {
                 x = valid ? in[0] : cx<C>((F)0, (F)0);
                 if constexpr (!kFwd) x = cswap(x);
             }
+            if constexpr (kR2C && WIN) {
+                {
+                    const C w = static_cast<const C*>(a.win)[0];
+                    x = cx<C>(mul_rn(x.x, w.x), mul_rn(x.y, w.y));
+                }
+            }
             v[0] = x;
             if constexpr (kR2C) {
                 sm[sidx(0)] = v[0];
@@ -512,6 +521,21 @@ struct TileWorker {
                                     for (int rho = 0; rho < G.R; ++rho) {
                                         C x = valid ? in[b + rho * (N / G.R)] : cx<C>((F)0, (F)0);
                                         v[u * G.R + rho] = kFwd ? x : cswap(x);
+                                    }
+                                }
+                            }
+                            if constexpr (kR2C && WIN) {  // STFT: window the frame as it is loaded
+                                {
+                                    const C* wp = static_cast<const C*>(a.win);
+#pragma unroll
+                                    for (int u = 0; u < NB; ++u) {
+                                        const int b = (kLast ? b_last : lt) + u * T;
+#pragma unroll
+                                        for (int rho = 0; rho < G.R; ++rho) {
+                                            const C w = __ldg(wp + b + rho * (N / G.R));
+                                            C& x = v[u * G.R + rho];
+                                            x = cx<C>(mul_rn(x.x, w.x), mul_rn(x.y, w.y));
+                                        }
                                     }
                                 }
                             }
@@ -669,9 +693,9 @@ struct TileWorker {
 };
 
 // ---------------------------------------------------------------- the kernel
-template <typename F, int P, int OP, int IL, int OL, bool GATHER = false>
+template <typename F, int P, int OP, int IL, int OL, bool GATHER = false, bool WIN = false>
 __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>::MINB) tile_kernel(const TileArgs a) {
-    using W = TileWorker<F, P, OP, IL, OL, 128, GATHER>;
+    using W = TileWorker<F, P, OP, IL, OL, 128, GATHER, WIN>;
     using Cfg = typename W::Cfg;
     using C = Cx<F>;
     constexpr int N = Cfg::N, TPC = Cfg::TPC;

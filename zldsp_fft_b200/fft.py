@@ -79,6 +79,12 @@ class Plan:
         C.check(self._lib.zlfft_exec_device(self.handle, op, in_layout, out_layout, in0, in1, out0, out1,
                                             int(batch), int(in_stride), int(out_stride), stream))
 
+    def stft(self, op, out_layout, signal, hop, window, out0, out1, n_frames, out_stride=0, stream=0):
+        """STFT frames of a device signal (zlfft_stft_device): frame f is
+        signal[f*hop : f*hop + N] * window, through forward or forward_sqr_mag."""
+        C.check(self._lib.zlfft_stft_device(self.handle, op, out_layout, signal, int(hop), window, out0, out1,
+                                            int(n_frames), int(out_stride), stream))
+
     def exec_host(self, op, in_layout, out_layout, in0, in1, out0, out1, batch=1):
         C.check(self._lib.zlfft_exec_host_batched(self.handle, op, in_layout, out_layout, in0, in1, out0, out1,
                                                   int(batch)))
