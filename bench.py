@@ -800,7 +800,125 @@ class Cfft10:
     cpu_threads = 1          # one transform: the reference runs it on one thread
 
 
-WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G, "mixed": Mixed, "cfft64": Cfft64, "cfft10": Cfft10}
+class Stft:
+    """STFT front end: a 2^27-sample real signal (U[-1, 1), seed 1006),
+    4096-point frames at hop 1024 (131,069 frames), periodic Hann window, power
+    spectrum (forward_sqr_mag) of every frame, in one zlfft_stft_device launch.
+    Algorithmic bytes: the signal read once plus the spectrogram written.
+    Beside it: the same spectrogram from frames cut and windowed by torch into a
+    buffer first (unfold * window), then the batched RFFT."""
+    name = "stft"
+    desc = ("STFT: 2^27-sample float signal, 4096-point Hann frames at hop 1024 (131,069 frames), "
+            "forward_sqr_mag, fused framing + window + RFFT")
+    l2 = "each step reads 512 MiB and writes 1.07 GB, > 10x L2 (no L2 flush needed)"
+    order, hop, total = 12, 1024, 1 << 27
+    dtype = "f32"
+
+    def __init__(self):
+        n = 1 << self.order
+        self.frame_n = n
+        self.nf = (self.total - n) // self.hop + 1
+        self.nb = n // 2 + 1
+        self.op_bytes = {"stft_sqr_mag": 4 * self.total + 4 * self.nb * self.nf}
+        self.bytes_per_step = self.op_bytes["stft_sqr_mag"]
+        self.dominant = "stft_sqr_mag"
+        self.batch = self.nf
+        self.host_in = None
+
+    def setup(self, device):
+        import torch
+        import zldsp_fft_b200 as Z
+        self.Z = Z
+        g = torch.Generator(device=device)
+        g.manual_seed(1006)
+        self.sig = (torch.rand(self.total, generator=g, device=device) * 2 - 1).contiguous()
+        t = torch.arange(self.frame_n, dtype=torch.float64, device=device)
+        self.win = (0.5 - 0.5 * torch.cos(2 * np.pi * t / self.frame_n)).float().contiguous()
+        self.out = torch.empty((self.nf, self.nb), dtype=torch.float32, device=device)
+        self.plan = Z.Plan(Z.R2C, self.order, np.float32, device=device)
+        torch.cuda.synchronize(device)
+
+    def ops(self, step):
+        Z = self.Z
+
+        def run(st):
+            self.plan.stft(Z.FORWARD_SQR_MAG, Z.AOS, self.sig.data_ptr(), self.hop, self.win.data_ptr(),
+                           self.out.data_ptr(), None, self.nf, stream=st)
+        return [("stft_sqr_mag", run)]
+
+    def take_launches(self):
+        return self.plan.take_launch_count()
+
+    def compare(self, stream, reps):
+        """The unfused path (frames materialised by torch, then the batched
+        RFFT) and the fused result's equality with it."""
+        import torch
+        Z = self.Z
+        ref_out = torch.empty_like(self.out)
+
+        def unfused():
+            with torch.cuda.stream(stream):
+                fr = (self.sig.unfold(0, self.frame_n, self.hop) * self.win).contiguous()
+                self.plan.exec_device(Z.FORWARD_SQR_MAG, Z.AOS, Z.AOS, fr.data_ptr(), None, ref_out.data_ptr(), None,
+                                      self.nf, stream=stream.cuda_stream)
+            return fr
+        for _ in range(2):
+            unfused()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            unfused()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        self.ops(0)[0][1](stream.cuda_stream)
+        torch.cuda.synchronize()
+        return {"unfused_frames_then_rfft": {"gbs": round(self.bytes_per_step / (ms / 1e3) / 1e9, 1), "ms": round(ms, 3)},
+                "fused_equals_unfused_bitwise": bool(torch.equal(self.out, ref_out))}
+
+    def cpu_sample_desc(self, frames):
+        return f"{frames} of {self.nf} frames: numpy framing + window, then the reference's forward_sqr_mag, median of 3"
+
+    def setup_e2e(self):
+        import torch
+        self.h_sig = self.sig.cpu().pin_memory()
+        self.h_out = torch.empty((self.nf, self.nb), dtype=torch.float32).pin_memory()
+        self.e2e_h2d = self.h_sig.numel() * 4
+        self.e2e_d2h = self.h_out.numel() * 4
+
+    def e2e_step(self):
+        import torch
+        st = torch.cuda.current_stream()
+        self.sig.copy_(self.h_sig, non_blocking=True)
+        self.ops(0)[0][1](st.cuda_stream)
+        self.h_out.copy_(self.out, non_blocking=True)
+        st.synchronize()
+
+    def cpu_run(self, frames, threads, kind):
+        from oracle import oracle as O
+        n, hop = self.frame_n, self.hop
+        frames = max(1, min(frames, self.nf))
+        rng = np.random.default_rng(1006)
+        sig = rng.uniform(-1, 1, (frames - 1) * hop + n).astype(np.float32)
+        win = (0.5 - 0.5 * np.cos(2 * np.pi * np.arange(n) / n)).astype(np.float32)
+        view = np.lib.stride_tricks.sliding_window_view(sig, n)[::hop]  # frames as views of the signal
+        out = np.empty((frames, self.nb), np.float32)
+        if kind == "reference":
+            plan = O.RefPlan("r2c", self.order, "f32", threads)
+            t0 = time.perf_counter()
+            fr = view * win  # the windowed copy a caller of forward_sqr_mag makes
+            plan.rfft_forward(fr, sqr_mag=True, out=out)
+            dt = time.perf_counter() - t0
+            plan.close()
+        else:
+            t0 = time.perf_counter()
+            O.rfft_forward_port(view * win, sqr_mag=True)
+            dt = time.perf_counter() - t0
+        return float(4 * ((frames - 1) * hop + n) + 4 * self.nb * frames), dt
+
+
+WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G, "mixed": Mixed, "cfft64": Cfft64, "cfft10": Cfft10, "stft": Stft}
 
 
 # ------------------------------------------------------------------ CPU baseline
