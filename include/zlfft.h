@@ -254,7 +254,8 @@ ZLFFT_API int zlfft_exec_mixed_device(const zlfft_desc* descs, size_t n, void* s
  *
  * Tuned parameters: for the multi-pass sizes (complex order >= 14) the scratch
  * chunk per pipeline, one or two chunk pipelines, TMA staging or direct loads
- * of the pass inputs, for RFFT forward the split as its own kernel or fused
+ * of the pass inputs, the first pass's output by TMA tensor stores or copied
+ * out by the threads, for RFFT forward the split as its own kernel or fused
  * into the last pass, and for CFFT<float> the computation form (plain or the
  * tensor-core split form); for the single-tile sizes, TMA staging or direct
  * loads. None of them changes the arithmetic of a form. Every plan created
@@ -270,6 +271,7 @@ typedef struct zlfft_tuning {
     int tma;            /* 1: inputs staged by TMA copies; 0: direct loads */
     int form;           /* ZLFFT_MODE_PLAIN or ZLFFT_MODE_TC_FP16 */
     int split_fused;    /* RFFT forward: 1 = split fused into the last pass, 0 = its own kernel */
+    int store_tma;      /* first pass: 1 = output by TMA tensor stores, 0 = copied out, -1 = default */
     double gbs;         /* measured algorithmic GB/s of the chosen plan (forward, AoS) */
     double gbs_default; /* of the default plan (48 MiB, 2 pipelines, TMA, plain) */
 } zlfft_tuning;

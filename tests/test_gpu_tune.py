@@ -60,7 +60,7 @@ def test_tuning_file_round_trip(tmp_path):
     assert Z.tuning_load(path) == 2
     for o in (13, 14):
         got = Z.tuning(Z.C2C, o, np.float32)
-        for k in ("chunk_mb", "streams", "tma", "form", "split_fused"):
+        for k in ("chunk_mb", "streams", "tma", "form", "split_fused", "store_tma"):
             assert got[k] == want[o][k], (o, k)
     # a file written on another GPU model is not applied here
     other = tmp_path / "other.txt"
@@ -85,7 +85,7 @@ def test_rfft_split_fused_into_last_pass(oracle, tmp_path, prec, dt):
     in FP64, including batches of several chunks."""
     name, sms = _this_gpu()
     pv = 0 if dt == np.float32 else 1
-    lines = [f"gpu {name} sms {sms}"] + [f"entry 1 {pv} {o} 48 2 1 0 1 0 0" for o in (15, 16, 17)]
+    lines = [f"gpu {name} sms {sms}"] + [f"entry 1 {pv} {o} 48 2 1 0 1 -1 0 0" for o in (15, 16, 17)]
     path = tmp_path / "fused.txt"
     path.write_text("\n".join(lines) + "\n")
     assert Z.tuning_load(str(path)) == 3
@@ -108,8 +108,33 @@ def test_rfft_split_fused_into_last_pass(oracle, tmp_path, prec, dt):
             ref = np.abs(oracle.rfft_fp64(x)) ** 2
             assert oracle.rel_l2(P, ref).max() <= 2 * tol
     # 300 frames of order 16 at a 16 MiB chunk: many chunks on both pipelines
-    path.write_text(f"gpu {name} sms {sms}\nentry 1 {pv} 16 16 2 1 0 1 0 0\n")
+    path.write_text(f"gpu {name} sms {sms}\nentry 1 {pv} 16 16 2 1 0 1 -1 0 0\n")
     assert Z.tuning_load(str(path)) == 1
     x = rng.uniform(-1, 1, (300, 1 << 16)).astype(dt)
     X = G.run_r2c(Z.Plan(Z.R2C, 16, dt), x, Z.AOS)
     assert oracle.rel_l2(X, oracle.rfft_fp64(x)).max() <= oracle.tolerance(16, prec)
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_first_pass_tma_store_on_and_off_give_the_same_bits(oracle, tmp_path, dt):
+    """The first multi-pass pass writes its output by TMA tensor stores of
+    swizzled boxes or by the threads; both give the same bits (FP32: the
+    oracle's), for pass radices 16 (order 20), 64 (14), 256 (16) and 512 (17)."""
+    name, sms = _this_gpu()
+    pv = 0 if dt == np.float32 else 1
+    rng = np.random.default_rng(123)
+    for order, batch in ((14, 33), (16, 9), (17, 3), (20, 1)):
+        n = 1 << order
+        x = (rng.uniform(-1, 1, (batch, n)) + 1j * rng.uniform(-1, 1, (batch, n))).astype(
+            np.complex64 if dt == np.float32 else np.complex128)
+        res = []
+        for store in (0, 1):
+            path = tmp_path / f"s{store}.txt"
+            path.write_text(f"gpu {name} sms {sms}\nentry 0 {pv} {order} 16 2 1 0 0 {store} 0 0\n")
+            Z.tuning_clear()
+            assert Z.tuning_load(str(path)) == 1
+            plan = Z.Plan(Z.C2C, order, dt)
+            res.append((G.run_c2c(plan, x, True), G.run_c2c(plan, x, False)))
+        assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1]), order
+        if dt == np.float32:
+            assert np.array_equal(res[1][0], oracle.cfft_port(x, True)), order

@@ -39,7 +39,8 @@ class Desc(ctypes.Structure):
 class Tuning(ctypes.Structure):
     """zlfft_tuning: the measured plan parameters of one transform size."""
     _fields_ = [("chunk_mb", ctypes.c_int), ("streams", ctypes.c_int), ("tma", ctypes.c_int), ("form", ctypes.c_int),
-                ("split_fused", ctypes.c_int), ("gbs", ctypes.c_double), ("gbs_default", ctypes.c_double)]
+                ("split_fused", ctypes.c_int), ("store_tma", ctypes.c_int), ("gbs", ctypes.c_double),
+                ("gbs_default", ctypes.c_double)]
 
 
 # every symbol include/zlfft.h declares

@@ -168,7 +168,7 @@ const TablesHolder& tables() {
 // Process-wide: (device, kind, precision, order) -> the plan parameters that
 // measured fastest there (zlfft_autotune), or that a tuning file recorded.
 struct TuneEntry {
-    int chunk_mb = 48, streams = 2, tma = 1, form = ZLFFT_MODE_PLAIN, split_fused = 0;
+    int chunk_mb = 48, streams = 2, tma = 1, form = ZLFFT_MODE_PLAIN, split_fused = 0, store_tma = -1;
     double gbs = 0, gbs_default = 0;
 };
 std::mutex g_tune_mu;
@@ -217,15 +217,16 @@ int tuning_load_impl(int device, const char* path, size_t* loaded) {
             same_gpu = (name == gname && sms == gsms);
             continue;
         }
-        int kind, prec, order, chunk, streams, tma, form, fused;
+        int kind, prec, order, chunk, streams, tma, form, fused, store;
         double gbs, gbs0;
-        if (sscanf(line, "entry %d %d %d %d %d %d %d %d %lf %lf", &kind, &prec, &order, &chunk, &streams, &tma, &form,
-                   &fused, &gbs, &gbs0) != 10)
+        if (sscanf(line, "entry %d %d %d %d %d %d %d %d %d %lf %lf", &kind, &prec, &order, &chunk, &streams, &tma,
+                   &form, &fused, &store, &gbs, &gbs0) != 11)
             continue;
         if (!same_gpu) continue;
         const bool ok = (kind == ZLFFT_C2C || kind == ZLFFT_R2C) && (prec == ZLFFT_F32 || prec == ZLFFT_F64) &&
                         order >= 0 && order <= zlfft::kPassMaxP + 1 && chunk >= 0 && chunk <= 4096 &&
                         (streams == 1 || streams == 2) && (tma == 0 || tma == 1) && (fused == 0 || fused == 1) &&
+                        (store >= -1 && store <= 1) &&
                         (form == ZLFFT_MODE_PLAIN ||
                          (form == ZLFFT_MODE_TC_FP16 && kind == ZLFFT_C2C && prec == ZLFFT_F32));
         if (!ok) continue;
@@ -235,6 +236,7 @@ int tuning_load_impl(int device, const char* path, size_t* loaded) {
         e.tma = tma;
         e.form = form;
         e.split_fused = fused;
+        e.store_tma = store;
         e.gbs = gbs;
         e.gbs_default = gbs0;
         std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -284,6 +286,7 @@ struct zlfft_plan_s {
     int use_tma = 1;        // TMA staging of kernel inputs (else direct loads)
     bool tc_form = false;   // 256-point passes in the tensor-core split form
     bool fuse_split = false;  // RFFT forward: split fused into the last pass (else its own kernel)
+    int store_tma = -1;       // first pass output by TMA tensor stores (-1: the precision's default)
     std::mutex mu;
 };
 
@@ -521,6 +524,7 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
             pa.tw = p->d_tw;
             pa.tctw = p->d_tctw ? static_cast<const char*>(p->d_tctw) + p->tctw_off[pi] * 2 * p->esize : nullptr;
             pa.err = p->d_err;
+            pa.tma_out = (p->store_tma < 0 ? p->prec == ZLFFT_F32 : p->store_tma == 1) ? 1 : 0;
             if (gfirst) {
                 pa.gin0 = gi0;
                 pa.gin1 = gi1;
@@ -801,6 +805,7 @@ int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layo
             pa.tw = p->d_tw;
             pa.tctw = p->d_tctw ? static_cast<const char*>(p->d_tctw) + p->tctw_off[pi] * 2 * p->esize : nullptr;
             pa.err = p->d_err;
+            pa.tma_out = (p->store_tma < 0 ? p->prec == ZLFFT_F32 : p->store_tma == 1) ? 1 : 0;
             const size_t eb = (pi == 0 && src_layout == ZLFFT_SOA) ? p->esize : cx;
             pa.tma = (p->use_tma && aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
                       (nb == 1 || ((size_t)src_stride * eb) % 16 == 0)) ? 1 : 0;
@@ -1337,6 +1342,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
             p->nlanes = te.streams;
             p->use_tma = te.tma;
             p->fuse_split = te.split_fused != 0;
+            p->store_tma = te.store_tma;
             if (mode == ZLFFT_MODE_TUNED && te.form == ZLFFT_MODE_TC_FP16) p->tc_form = true;
         }
         if (mode == ZLFFT_MODE_TC_FP16) p->tc_form = true;
@@ -1633,6 +1639,7 @@ int time_candidate(int device, int kind, int prec, int order, const TuneEntry& c
     p->nlanes = c.streams;
     p->use_tma = c.tma;
     p->fuse_split = c.split_fused != 0;
+    p->store_tma = c.store_tma;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1700,16 +1707,18 @@ int autotune_impl(int device, int kind, int prec, size_t lo, size_t hi) {
                 for (int chunk : {16, 32, 48, 96, 192})
                     for (int streams : {1, 2})
                         for (int tma : {0, 1})
-                            for (int fused : {0, 1}) {
-                                if (fused && kind != ZLFFT_R2C) continue;
-                                TuneEntry c;
-                                c.chunk_mb = chunk;
-                                c.streams = streams;
-                                c.tma = tma;
-                                c.form = form;
-                                c.split_fused = fused;
-                                cands.push_back(c);
-                            }
+                            for (int fused : {0, 1})
+                                for (int store : {0, 1}) {
+                                    if (fused && kind != ZLFFT_R2C) continue;
+                                    TuneEntry c;
+                                    c.chunk_mb = chunk;
+                                    c.streams = streams;
+                                    c.tma = tma;
+                                    c.form = form;
+                                    c.split_fused = fused;
+                                    c.store_tma = store;
+                                    cands.push_back(c);
+                                }
             }
         } else {
             for (int tma : {1, 0}) {
@@ -1727,8 +1736,10 @@ int autotune_impl(int device, int kind, int prec, size_t lo, size_t hi) {
             rc = time_candidate(device, kind, prec, (int)order, c, d_in, d_out, batch, st, &ms);
             if (rc) break;
             const double gbs = (double)batch * (double)(per_in + per_out) / (ms * 1e6);
+            const int store_default = prec == ZLFFT_F32 ? 1 : 0;
             const bool is_default = c.form == ZLFFT_MODE_PLAIN && c.tma == 1 && c.split_fused == 0 &&
-                                    (c.chunk_mb == 0 || (c.chunk_mb == 48 && c.streams == 2));
+                                    (c.chunk_mb == 0 || (c.chunk_mb == 48 && c.streams == 2 &&
+                                                         c.store_tma == store_default));
             if (is_default) def_gbs = gbs;
             if (gbs > best_gbs) {
                 best_gbs = gbs;
@@ -1766,6 +1777,7 @@ int zlfft_tuning_get(int device, int kind, int precision, size_t order, zlfft_tu
     out->tma = e.tma;
     out->form = e.form;
     out->split_fused = e.split_fused;
+    out->store_tma = e.store_tma;
     out->gbs = e.gbs;
     out->gbs_default = e.gbs_default;
     return ZLFFT_OK;
@@ -1780,16 +1792,17 @@ int zlfft_tuning_save(int device, const char* path) {
     if (rc) return rc;
     FILE* f = fopen(path, "w");
     if (!f) return fail(ZLFFT_ERR_INVALID_ARG, "cannot write tuning file %s", path);
-    fprintf(f, "# zlfft tuning table: entry kind precision order chunk_mb streams tma form split_fused gbs "
-               "gbs_default\n");
+    fprintf(f, "# zlfft tuning table: entry kind precision order chunk_mb streams tma form split_fused store_tma "
+               "gbs gbs_default\n");
     fprintf(f, "gpu %s sms %d\n", name.c_str(), sms);
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         for (const auto& kv : g_tune) {
             if (std::get<0>(kv.first) != device) continue;
             const TuneEntry& e = kv.second;
-            fprintf(f, "entry %d %d %d %d %d %d %d %d %.1f %.1f\n", std::get<1>(kv.first), std::get<2>(kv.first),
-                    std::get<3>(kv.first), e.chunk_mb, e.streams, e.tma, e.form, e.split_fused, e.gbs, e.gbs_default);
+            fprintf(f, "entry %d %d %d %d %d %d %d %d %d %.1f %.1f\n", std::get<1>(kv.first), std::get<2>(kv.first),
+                    std::get<3>(kv.first), e.chunk_mb, e.streams, e.tma, e.form, e.split_fused, e.store_tma, e.gbs,
+                    e.gbs_default);
         }
     }
     if (fclose(f) != 0) return fail(ZLFFT_ERR_INVALID_ARG, "writing %s failed", path);

@@ -175,6 +175,19 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* map, int x, i
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
         : "memory");
 }
+// 2-D tiled tensor copy shared -> global (no multicast), in this thread's
+// current bulk group; bulk_commit closes the group, bulk_wait_read0 waits
+// until every committed group has finished reading shared memory, and
+// bulk_wait0 until every committed group has completed.
+__device__ __forceinline__ void tma_store_2d(const void* map, int x, int y, const void* src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // Orders this thread's earlier generic-proxy shared-memory accesses before
 // later async-proxy (TMA) accesses of shared memory. Every thread that read a
 // staging buffer executes it before the barrier after which the buffer is

@@ -173,6 +173,26 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
     a.tma = (SPLIT == 0 && tma_enabled && a.tma && !(Cfg::FIRST && a.gin0) && encode_pass_maps<F, P, PI, IL2>(a, maps))
                 ? 1
                 : 0;
+    // a.tma_out on entry: the plan asks for tensor stores of the first pass's output
+    const bool want_store = a.tma_out != 0;
+    a.tma_out = 0;
+    if constexpr (Cfg::kStoreTMA) {
+        // first pass into dense scratch: rows of R points, one per unit of every transform
+        PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+        if (want_store && tma_enabled && enc && a.out_stride == Cfg::N &&
+            reinterpret_cast<uintptr_t>(a.out0) % 1024 == 0) {
+            const CUtensorMapDataType dt =
+                sizeof(F) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+            const cuuint64_t dims[2] = {(cuuint64_t)Cfg::R * 2, (cuuint64_t)a.batch * Cfg::UNITS};
+            const cuuint64_t strides[1] = {(cuuint64_t)Cfg::R * 2 * sizeof(F)};
+            const cuuint32_t box[2] = {(cuuint32_t)(Cfg::CPB * 2), (cuuint32_t)Cfg::UPC};
+            const cuuint32_t estr[2] = {1, 1};
+            if (enc(&maps.mo, dt, 2, a.out0, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+                a.tma_out = 1;
+        }
+    }
     static const int blocks_per_sm = [kern]() {
         if (Cfg::SMEM > 48 * 1024)
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);

@@ -86,8 +86,16 @@ struct PassCfg {
     // The next item's input (a box of UPC units x R positions) is prefetched
     // by one 3-D tensor copy per 256 positions while the current item computes.
     static constexpr int RB = R < 256 ? R : 256;  // positions per box
-    static constexpr bool kTMA = SOFF + SBYTES + 16 <= 200 * 1024;
-    static constexpr size_t SMEM = kTMA ? SOFF + SBYTES + 16 : XBYTES;
+    static constexpr bool kTMA = SOFF + SBYTES + 16 + 1024 <= 200 * 1024;
+    // (+1024: the buffers start at the first 1024-byte boundary of the dynamic
+    // shared memory, as the swizzled output boxes of the first pass require)
+    static constexpr size_t SMEM = (kTMA ? SOFF + SBYTES + 16 : XBYTES) + 1024;
+    // First pass: the CTA's output block (UPC units x R contiguous points) is
+    // written by tensor stores of 128-byte-swizzled boxes, 128 bytes of points
+    // x UPC units each, staged in the exchange buffer.
+    static constexpr int CPB = 128 / (int)sizeof(C);  // points per box row
+    static constexpr bool kStoreTMA = (L_IN == 1) && !LAST && (R % CPB == 0) && (UPC % 8 == 0) &&
+                                      (size_t)UPC * R * sizeof(C) <= XBYTES;
     static constexpr int UNITS = N / R;            // units per transform
     static constexpr int CPT = UNITS / UPC;        // CTAs (work items) per transform
     static constexpr int MINB = (65536 / (THREADS * 96)) > 0 ? (65536 / (THREADS * 96)) : 1;
@@ -107,6 +115,7 @@ struct PassArgs {
     const void* tw;        // unified table T[t] = W_N^t, t < 3N/4 (tensor-core passes)
     const void* tctw;      // this pass's tensor-core twiddles when L_in > 1 (zlfft_tc_pass.cuh)
     const void* rw;        // RFFT split twiddle pairs (last pass with the split fused)
+    int tma_out;           // first pass: the output map (PassMaps::mo) is valid, store by TMA
     int* err;              // device error word (kDevErrWaitTimeout on a timed-out wait)
     int tma;               // the tensor maps describe the input (else direct loads)
     // Gathered transforms (mixed batches): the first pass reads transform t
@@ -123,6 +132,7 @@ struct PassArgs {
 struct PassMaps {
     CUtensorMap m0;
     CUtensorMap m1;
+    CUtensorMap mo;  // first pass: the output, as rows of R points (one row per unit)
 };
 
 // Unit of slot u in work item ib of a last pass with the RFFT split fused:
@@ -160,7 +170,10 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
     constexpr int OL2 = Cfg::LAST ? OL : (int)kAoS;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* sm = reinterpret_cast<C*>(smem_raw);
+    // first 1024-byte boundary, as an offset into the shared array (keeps the
+    // pointer in the shared address space for the compiler)
+    unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    C* sm = reinterpret_cast<C*>(smem);
     const int u = (int)threadIdx.x % UPC;
     const int tb = (int)threadIdx.x / UPC;
     const C* tws = static_cast<const C*>(a.tws);
@@ -169,8 +182,9 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
     // ---- TMA staging: [pos][u] unpadded (SoA: a re plane then an im plane)
     constexpr bool kSoAIn = (IL2 == kSoA);
     constexpr int CMP = kSoAIn ? 1 : 2;  // scalars per unit in the map's innermost dimension
-    C* stage = reinterpret_cast<C*>(smem_raw + Cfg::SOFF);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::SOFF + Cfg::SBYTES);
+    C* stage = reinterpret_cast<C*>(smem + Cfg::SOFF);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + Cfg::SOFF + Cfg::SBYTES);
+    const bool store_tma = Cfg::kStoreTMA && a.tma_out;
     static_assert(SPLIT == 0 || (Cfg::LAST && FWD && L_IN > 1 && Cfg::UPC >= 2), "split fusion: RFFT forward last pass");
     const bool use_tma = Cfg::kTMA && a.tma && SPLIT == 0;
     auto issue = [&](long long it) {  // one thread issues the item's box copies
@@ -202,6 +216,9 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
     uint32_t phase = 0;
 
     for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+        // the previous item's output stores have read the exchange buffer before
+        // anyone writes it again (the first write follows a barrier)
+        if (store_tma && threadIdx.x == 0) bulk_wait_read0();
         const long long tr = item / Cfg::CPT;
         const int ib = (int)(item % Cfg::CPT);
         const int U = SPLIT ? split_unit<L_IN, UPC>(ib, u) : ib * UPC + u;
@@ -214,6 +231,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                 if (__syncthreads_or(!ok)) {  // bounded wait ran out: report and leave
                     if (threadIdx.x == 0) atomicOr(a.err, kDevErrWaitTimeout);
                     mbar_wait(bar, phase);
+                    if (store_tma && threadIdx.x == 0) bulk_wait0();
                     return;
                 }
                 phase ^= 1u;
@@ -289,6 +307,39 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                         }
                         __syncthreads();
                     } else if constexpr (L_IN == 1) {
+                        if constexpr (Cfg::kStoreTMA) {
+                            if (store_tma) {
+                                // first pass: the CTA's output block (UPC units x R contiguous
+                                // points) as R / CPB boxes [unit][CPB points], 128-byte swizzled
+                                // (16-byte chunk c of unit row u at chunk c ^ (u & 7)), written by
+                                // tensor stores while the next item computes
+                                constexpr int CPB = Cfg::CPB;
+                                __syncthreads();
+#pragma unroll
+                                for (int i = 0; i < NB; ++i) {
+                                    const int b = tb + i * T;
+#pragma unroll
+                                    for (int s = 0; s < G.R; ++s) {
+                                        const int pos = b + group_mu(G, s) * ELL;
+                                        const uint32_t cb = (uint32_t)((pos % CPB) * (int)sizeof(C));
+                                        const uint32_t off = (uint32_t)(pos / CPB) * (uint32_t)(UPC * 128) +
+                                                             (uint32_t)u * 128u + ((((cb >> 4) ^ (uint32_t)(u & 7))) << 4) +
+                                                             (cb & 15u);
+                                        *reinterpret_cast<C*>(smem + off) = v[i * G.R + s];
+                                    }
+                                }
+                                fence_proxy_async_smem();  // generic writes before the async-proxy reads
+                                __syncthreads();
+                                if (threadIdx.x == 0) {
+                                    const int y = (int)(tr * Cfg::UNITS + (U - u));
+#pragma unroll 1
+                                    for (int bx = 0; bx < R / CPB; ++bx)
+                                        tma_store_2d(&maps.mo, bx * CPB * 2, y, smem + (size_t)bx * UPC * 128);
+                                    bulk_commit();
+                                }
+                                return;
+                            }
+                        }
                         // first pass: each unit's outputs are contiguous; stage them and copy
                         // the CTA's block (UPC units x R) out with consecutive threads on
                         // consecutive elements.
@@ -402,6 +453,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
         }
         // shared memory is rewritten by the next item's first exchange only after a barrier
     }
+    if (store_tma && threadIdx.x == 0) bulk_wait0();  // stores done before the CTA's shared memory goes
 }
 
 // ---------------------------------------------------------------- RFFT split / pre-step

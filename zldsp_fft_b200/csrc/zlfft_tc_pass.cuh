@@ -94,8 +94,9 @@ __global__ void __launch_bounds__(256, 3) tc_pass_kernel(const PassArgs a, const
     constexpr bool UMAJ = Cfg::kUnitMajorB;
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    unsigned char* smem =
-        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    // first 1024-byte boundary, as an offset into the shared array (keeps the
+    // pointer in the shared address space for the compiler)
+    unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     C* stage = reinterpret_cast<C*>(smem + Cfg::STAGE_OFF);
     unsigned char* a_tile = smem + Cfg::A_OFF;
     unsigned char* b_tile = smem + Cfg::B_OFF;

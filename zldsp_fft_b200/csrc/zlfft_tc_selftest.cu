@@ -15,8 +15,7 @@ __global__ void __launch_bounds__(128) tc_dft16_selftest_kernel(const float2* __
                                                                   const float2* __restrict__ tw16, int* err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // the swizzle pattern is a function of the address bits: align the tiles to 1024 bytes
-    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
-                                                           ~uintptr_t(1023));
+    unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     unsigned char* a_tile = smem;
     unsigned char* b_tile = smem + 16384;
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 20480);
