@@ -149,7 +149,7 @@ struct TileCfg {
     static constexpr int NG = tile_num_groups(P);
     // Register budget: enough resident CTAs for ~96 registers per thread in
     // FP32 (the last group's 15 complex twiddles stay in registers), ~128 in FP64.
-    static constexpr int REGS = sizeof(F) == 4 ? 96 : 128;
+    static constexpr int REGS = sizeof(F) == 4 ? (((OP == kC2CFwd || OP == kC2CBwd) && P >= 10) ? 128 : 96) : 128;
     static constexpr int MINB = (65536 / (THREADS * REGS)) > 0 ? (65536 / (THREADS * REGS)) : 1;
 };
 
