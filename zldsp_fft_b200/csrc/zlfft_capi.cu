@@ -1025,6 +1025,12 @@ struct zlfft_mixed_s {
     int n_items[2] = {0, 0};
     int* d_counter = nullptr;  // one work-list counter per precision
     cudaStream_t cap_stream = nullptr;
+    // persistent schedule: the multi-pass and large-tile groups run on these
+    // streams (forked from the caller's stream, joined back) beside the
+    // persistent launch
+    static constexpr int kSideStreams = 2;
+    cudaStream_t side[kSideStreams] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[kSideStreams] = {nullptr, nullptr};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     size_t graph_launches = 0;  // kernels recorded in the graph
@@ -1041,6 +1047,11 @@ void mixed_release(zlfft_mixed m) {
         if (m->graph_exec) cudaGraphExecDestroy(m->graph_exec);
         if (m->graph) cudaGraphDestroy(m->graph);
         if (m->cap_stream) cudaStreamDestroy(m->cap_stream);
+        for (int i = 0; i < zlfft_mixed_s::kSideStreams; ++i) {
+            if (m->side[i]) cudaStreamDestroy(m->side[i]);
+            if (m->ev_join[i]) cudaEventDestroy(m->ev_join[i]);
+        }
+        if (m->ev_fork) cudaEventDestroy(m->ev_fork);
         if (m->d_mem) cudaFree(m->d_mem);
     }
     for (zlfft_plan p : m->plans) release(p);
@@ -1102,12 +1113,28 @@ int mixed_run_group(zlfft_mixed_s* m, const MixedGroupHost& g, cudaStream_t st) 
 
 int mixed_run(zlfft_mixed_s* m, int schedule, cudaStream_t st) {
     const bool persistent = schedule != ZLFFT_SCHED_PER_ORDER;
-    for (const MixedGroupHost& g : m->groups) {
-        if (persistent && mixed_in_persistent(g)) continue;
-        int rc = mixed_run_group(m, g, st);
-        if (rc) return rc;
+    if (!persistent) {  // the baseline: one batched launch (or pipeline) per group, in order
+        for (const MixedGroupHost& g : m->groups) {
+            int rc = mixed_run_group(m, g, st);
+            if (rc) return rc;
+        }
+        return ZLFFT_OK;
     }
-    if (!persistent) return ZLFFT_OK;
+    // The groups outside the persistent kernel (largest first) are dealt to the
+    // side streams, so groups of different orders overlap each other's tails
+    // and the persistent launch on the caller's stream.
+    int big = 0;
+    for (const MixedGroupHost& g : m->groups) big += mixed_in_persistent(g) ? 0 : 1;
+    if (big) {
+        ZL_CUDA(cudaEventRecord(m->ev_fork, st));
+        for (int i = 0; i < zlfft_mixed_s::kSideStreams; ++i) ZL_CUDA(cudaStreamWaitEvent(m->side[i], m->ev_fork, 0));
+        int k = 0;
+        for (const MixedGroupHost& g : m->groups) {
+            if (mixed_in_persistent(g)) continue;
+            int rc = mixed_run_group(m, g, m->side[k++ % zlfft_mixed_s::kSideStreams]);
+            if (rc) return rc;
+        }
+    }
     for (int pr = 0; pr < 2; ++pr) {
         if (!m->n_items[pr]) continue;
         ZL_CUDA(cudaMemsetAsync(m->d_counter + pr, 0, sizeof(int), st));
@@ -1117,6 +1144,12 @@ int mixed_run(zlfft_mixed_s* m, int schedule, cudaStream_t st) {
                                                           m->d_counter + 1, st, m->num_sms);
         if (e != cudaSuccess) return cuda_fail(e, "persistent mixed launch");
         ++m->launches;
+    }
+    if (big) {
+        for (int i = 0; i < zlfft_mixed_s::kSideStreams; ++i) {
+            ZL_CUDA(cudaEventRecord(m->ev_join[i], m->side[i]));
+            ZL_CUDA(cudaStreamWaitEvent(st, m->ev_join[i], 0));
+        }
     }
     return ZLFFT_OK;
 }
@@ -1264,6 +1297,11 @@ int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int d
     }
     if (e == cudaSuccess) e = cudaMemset(m->d_counter, 0, 2 * sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&m->cap_stream, cudaStreamNonBlocking);
+    for (int i = 0; i < zlfft_mixed_s::kSideStreams && e == cudaSuccess; ++i) {
+        e = cudaStreamCreateWithFlags(&m->side[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->ev_join[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         mixed_release(m);
         return cuda_fail(e, "mixed batch set-up");
