@@ -65,6 +65,9 @@ typedef struct zlfft_plan_s* zlfft_plan;
 #define ZLFFT_MODE_TC_BF16 2 /* split 3-way BF16 */
 #define ZLFFT_MODE_TC_TF32 3 /* 3xTF32 */
 #define ZLFFT_MODE_TUNED 4   /* the autotuned plan of this device and size (see zlfft_autotune) */
+#define ZLFFT_MODE_FAST 5    /* plain CUDA-core form whose multi-pass radix-16 groups build their
+                                twiddles from two table values (fewer loads): within the FP bar,
+                                not bit-identical to the reference; single-tile sizes as PLAIN */
 
 /* Create a plan for one transform size.
  * Replaces the constructors CFFT<F>::CFFT(size_t order)
@@ -256,8 +259,8 @@ ZLFFT_API int zlfft_exec_mixed_device(const zlfft_desc* descs, size_t n, void* s
  * chunk per pipeline, one or two chunk pipelines, TMA staging or direct loads
  * of the pass inputs, the first pass's output by TMA tensor stores or copied
  * out by the threads, for RFFT forward the split as its own kernel or fused
- * into the last pass, and for CFFT<float> the computation form (plain or the
- * tensor-core split form); for the single-tile sizes, TMA staging or direct
+ * into the last pass, and the computation form (plain, fast-twiddle, and for
+ * CFFT<float> the tensor-core split form); for the single-tile sizes, TMA staging or direct
  * loads. None of them changes the arithmetic of a form. Every plan created
  * afterwards on that device and size uses the tuned chunk, pipelines and
  * staging; plans created with ZLFFT_MODE_TUNED also take the tuned form
@@ -269,7 +272,7 @@ typedef struct zlfft_tuning {
     int chunk_mb;       /* scratch per chunk pipeline buffer, MiB (0: single-tile size) */
     int streams;        /* chunk pipelines, 1 or 2 */
     int tma;            /* 1: inputs staged by TMA copies; 0: direct loads */
-    int form;           /* ZLFFT_MODE_PLAIN or ZLFFT_MODE_TC_FP16 */
+    int form;           /* ZLFFT_MODE_PLAIN, ZLFFT_MODE_FAST or ZLFFT_MODE_TC_FP16 */
     int split_fused;    /* RFFT forward: 1 = split fused into the last pass, 0 = its own kernel */
     int store_tma;      /* first pass: 1 = output by TMA tensor stores, 0 = copied out, -1 = default */
     double gbs;         /* measured algorithmic GB/s of the chosen plan (forward, AoS) */

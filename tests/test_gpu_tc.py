@@ -83,3 +83,33 @@ def test_tc_mode_rejected_where_not_built():
     assert lib.zlfft_plan_create(ctypes.byref(h), Z.R2C, Z.F32, 12, Z.MODE_TC_FP16, -1) == Z._capi.ERR_UNSUPPORTED
     assert lib.zlfft_plan_create(ctypes.byref(h), Z.C2C, Z.F64, 16, Z.MODE_TC_FP16, -1) == Z._capi.ERR_UNSUPPORTED
     assert lib.zlfft_plan_create(ctypes.byref(h), Z.C2C, Z.F32, 16, Z.MODE_TC_BF16, -1) == Z._capi.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("prec,ft,ct", [("f32", np.float32, np.complex64), ("f64", np.float64, np.complex128)])
+@pytest.mark.parametrize("order", [14, 15, 16, 17, 20])
+def test_fast_twiddle_form_within_tolerance(oracle, prec, ft, ct, order):
+    """ZLFFT_MODE_FAST (multi-pass radix-16 groups with twiddles built from two
+    table values): CFFT both directions, RFFT forward / sqr_mag / backward,
+    within the FP bar of the FP64 oracle; the form really runs (its bits
+    differ from the plain form's)."""
+    from tests import gpu_util as G
+    rng = np.random.default_rng(700 + order)
+    n = 1 << order
+    batch = 3 if order <= 17 else 1
+    tol = oracle.tolerance(order, prec)
+    x = (rng.uniform(-1, 1, (batch, n)) + 1j * rng.uniform(-1, 1, (batch, n))).astype(ct)
+    fast = Z.Plan(Z.C2C, order, ft, mode=Z.MODE_FAST)
+    y = G.run_c2c(fast, x, True)
+    assert oracle.rel_l2(y, oracle.cfft_fp64(x)).max() <= tol
+    assert not np.array_equal(y, G.run_c2c(Z.Plan(Z.C2C, order, ft), x, True))
+    z = G.run_c2c(fast, y, False)
+    assert oracle.rel_l2(z, oracle.cfft_fp64(y, False)).max() <= tol
+    xr = rng.uniform(-1, 1, (batch, n)).astype(ft)
+    rf = Z.Plan(Z.R2C, order, ft, mode=Z.MODE_FAST)
+    X = G.run_r2c(rf, xr)
+    assert oracle.rel_l2(X, oracle.rfft_fp64(xr)).max() <= tol
+    Pw = G.run_r2c(rf, xr, sqr_mag=True)
+    assert oracle.rel_l2(Pw, np.abs(oracle.rfft_fp64(xr)) ** 2).max() <= 2 * tol
+    back = G.run_c2r(rf, X.astype(ct))
+    assert oracle.rel_l2(back, oracle.rfft_backward_fp64(X.astype(ct))).max() <= tol
+    assert fast.device_status() == 0 and rf.device_status() == 0

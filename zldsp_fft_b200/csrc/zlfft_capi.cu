@@ -227,7 +227,7 @@ int tuning_load_impl(int device, const char* path, size_t* loaded) {
                         order >= 0 && order <= zlfft::kPassMaxP + 1 && chunk >= 0 && chunk <= 4096 &&
                         (streams == 1 || streams == 2) && (tma == 0 || tma == 1) && (fused == 0 || fused == 1) &&
                         (store >= -1 && store <= 1) &&
-                        (form == ZLFFT_MODE_PLAIN ||
+                        (form == ZLFFT_MODE_PLAIN || form == ZLFFT_MODE_FAST ||
                          (form == ZLFFT_MODE_TC_FP16 && kind == ZLFFT_C2C && prec == ZLFFT_F32));
         if (!ok) continue;
         TuneEntry e;
@@ -285,6 +285,7 @@ struct zlfft_plan_s {
     int nlanes = 2;         // chunk pipelines
     int use_tma = 1;        // TMA staging of kernel inputs (else direct loads)
     bool tc_form = false;   // 256-point passes in the tensor-core split form
+    bool fast_form = false; // multi-pass radix-16 groups with fast twiddles (ZLFFT_MODE_FAST)
     bool fuse_split = false;  // RFFT forward: split fused into the last pass (else its own kernel)
     int store_tma = -1;       // first pass output by TMA tensor stores (-1: the precision's default)
     std::mutex mu;
@@ -437,6 +438,10 @@ zlfft::PassLaunchFn pick_pass(const zlfft_plan_s* p, int pi, bool fwd, int li, i
         if (f) return f;
     }
     const zlfft::PassTable& t = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
+    if (p->fast_form && li == ZLFFT_AOS && lo == ZLFFT_AOS) {
+        zlfft::PassLaunchFn f = t.fast[P - zlfft::kPassMinP][pi][fwd ? 1 : 0];
+        if (f) return f;
+    }
     return t.fn[P - zlfft::kPassMinP][pi][fwd ? 1 : 0][li][lo];
 }
 
@@ -1346,7 +1351,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
     if (order > 30) return fail(ZLFFT_ERR_INVALID_ARG, "order %zu out of range", order);
     if (kind == ZLFFT_R2C && order < 1)
         return fail(ZLFFT_ERR_INVALID_ARG, "RFFT order must be >= 1 (the reference underflows at 0)");
-    if (mode != ZLFFT_MODE_PLAIN && mode != ZLFFT_MODE_TC_FP16 && mode != ZLFFT_MODE_TUNED)
+    if (mode != ZLFFT_MODE_PLAIN && mode != ZLFFT_MODE_TC_FP16 && mode != ZLFFT_MODE_TUNED && mode != ZLFFT_MODE_FAST)
         return fail(ZLFFT_ERR_UNSUPPORTED, "mode %d not available", mode);
     if (mode == ZLFFT_MODE_TC_FP16 && (kind != ZLFFT_C2C || precision != ZLFFT_F32))
         return fail(ZLFFT_ERR_UNSUPPORTED, "the tensor-core split form is built for CFFT<float>");
@@ -1382,8 +1387,10 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
             p->fuse_split = te.split_fused != 0;
             p->store_tma = te.store_tma;
             if (mode == ZLFFT_MODE_TUNED && te.form == ZLFFT_MODE_TC_FP16) p->tc_form = true;
+            if (mode == ZLFFT_MODE_TUNED && te.form == ZLFFT_MODE_FAST) p->fast_form = true;
         }
         if (mode == ZLFFT_MODE_TC_FP16) p->tc_form = true;
+        if (mode == ZLFFT_MODE_FAST) p->fast_form = true;
     }
     cudaError_t e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
@@ -1740,7 +1747,7 @@ int autotune_impl(int device, int kind, int prec, size_t lo, size_t hi) {
         std::vector<TuneEntry> cands;
         const bool tc_ok = kind == ZLFFT_C2C && prec == ZLFFT_F32 && cfft_order >= zlfft::kPassMinP;
         if (cfft_order >= zlfft::kPassMinP) {
-            for (int form : {ZLFFT_MODE_PLAIN, ZLFFT_MODE_TC_FP16}) {
+            for (int form : {ZLFFT_MODE_PLAIN, ZLFFT_MODE_FAST, ZLFFT_MODE_TC_FP16}) {
                 if (form == ZLFFT_MODE_TC_FP16 && !tc_ok) continue;
                 for (int chunk : {16, 32, 48, 96, 192})
                     for (int streams : {1, 2})

@@ -109,6 +109,8 @@ struct PassTable {
     // [order - kPassMinP][0: RFFT forward, 1: forward_sqr_mag][output layout]: the
     // last pass with the RFFT split fused (the N/2-point spectrum never leaves the CTA)
     PassLaunchFn split[kPassMaxP - kPassMinP + 1][2][2];
+    // [order - kPassMinP][pass][fwd]: the fast-twiddle form, AoS in and out
+    PassLaunchFn fast[kPassMaxP - kPassMinP + 1][kMaxPasses][2];
 };
 
 // cuTensorMapEncodeTiled, reached through the runtime's driver entry point
@@ -156,10 +158,10 @@ bool encode_pass_maps(const PassArgs& a, PassMaps& m) {
     return true;
 }
 
-template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0>
+template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0, bool FAST = false>
 cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = PassCfg<F, P, PI>;
-    auto kern = pass_kernel<F, P, PI, FWD, IL, OL, SPLIT>;
+    auto kern = pass_kernel<F, P, PI, FWD, IL, OL, SPLIT, FAST>;
     constexpr int IL2 = Cfg::FIRST ? IL : (int)kAoS;
     PassArgs a = a_in;
     PassMaps maps;
@@ -249,6 +251,21 @@ void fill_pass_order(PassTable& t) {
     fill_pass_one<F, P, 0>(t);
     fill_pass_one<F, P, 1>(t);
     if constexpr (pass_count(P) > 2) fill_pass_one<F, P, 2>(t);
+    // fast-twiddle form (AoS): the direction only matters on the first and last pass
+    constexpr int NP = pass_count(P);
+    [&]<int... PIs>(std::integer_sequence<int, PIs...>) {
+        (
+            [&] {
+                auto& fe = t.fast[P - kPassMinP][PIs];
+                if constexpr (PIs == 0 || PIs + 1 == NP) {
+                    fe[1] = launch_pass<F, P, PIs, true, kAoS, kAoS, 0, true>;
+                    fe[0] = launch_pass<F, P, PIs, false, kAoS, kAoS, 0, true>;
+                } else {
+                    fe[0] = fe[1] = launch_pass<F, P, PIs, true, kAoS, kAoS, 0, true>;
+                }
+            }(),
+            ...);
+    }(std::make_integer_sequence<int, NP>{});
     // last pass with the RFFT split fused: [forward | sqr_mag][output layout]
     constexpr int PL = pass_count(P) - 1;
     auto& sp = t.split[P - kPassMinP];

@@ -274,7 +274,8 @@ def tuning(kind: int, order: int, dtype=np.float32, device: int = -1):
         return None
     C.check(rc)
     return {"chunk_mb": t.chunk_mb, "streams": t.streams, "tma": t.tma,
-            "form": "tc_fp16" if t.form == C.MODE_TC_FP16 else "plain", "split_fused": t.split_fused,
+            "form": {C.MODE_TC_FP16: "tc_fp16", C.MODE_FAST: "fast"}.get(t.form, "plain"),
+            "split_fused": t.split_fused,
             "store_tma": t.store_tma,
             "gbs": t.gbs, "gbs_default": t.gbs_default}
 
