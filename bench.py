@@ -37,6 +37,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Batched FFT HBM GB/s (% of roofline), TC-split vs plain FP32 at equal error"
+FORMS = {
+    "plain": "plain (the reference's Stockham radix-4/8 DIT on CUDA cores, bit-identical results)",
+    "fast": "fast-twiddle plain form: CUDA cores, radix-16 groups' twiddles from two table values per butterfly",
+    "tc": "tensor-core split FP16 hi/lo, FP32 accumulate (256-point passes), plain elsewhere",
+    "tuned": "autotuned per order among plain, fast-twiddle and tensor-core split forms (see schedules)",
+}
 
 
 # ------------------------------------------------------------------ helpers
@@ -270,11 +276,12 @@ class Cfft2G:
     total = 1 << 28  # complex elements per order (2 GiB)
     dtype = "f32"
 
-    def __init__(self, total_log2=28, form="plain"):
+    def __init__(self, total_log2=28, form="tuned"):
         self.total = 1 << total_log2
         self.form = form
-        if form == "tc":
-            self.desc = self.desc + ", tensor-core split FP16 hi/lo form"
+        self.desc = self.desc + {"tc": ", tensor-core split FP16 hi/lo form", "fast": ", fast-twiddle form",
+                                 "plain": ", plain form (the reference's arithmetic, bit-identical)",
+                                 "tuned": ", autotuned form per order"}[form]
         self.op_bytes = {}
         for o in self.orders:
             for d in ("fwd", "bwd"):
@@ -286,7 +293,12 @@ class Cfft2G:
         import torch
         import zldsp_fft_b200 as Z
         self.Z = Z
-        mode = Z.MODE_TC_FP16 if self.form == "tc" else Z.MODE_PLAIN
+        mode = {"tc": Z.MODE_TC_FP16, "fast": Z.MODE_FAST, "plain": Z.MODE_PLAIN, "tuned": Z.MODE_TUNED}[self.form]
+        self.tuning = None
+        if self.form == "tuned":  # set-up, outside the timed region
+            for o in self.orders:
+                Z.autotune(Z.C2C, o, o, np.float32, device=device)
+            self.tuning = {f"order{o}": Z.tuning(Z.C2C, o, np.float32, device=device) for o in self.orders}
         self.plans = {o: Z.Plan(Z.C2C, o, np.float32, mode=mode, device=device) for o in self.orders}
         g = torch.Generator(device=device)
         g.manual_seed(1003)
@@ -322,7 +334,7 @@ class Cfft2G:
         import torch
         Z = self.Z
         out = {}
-        for form, mode in (("plain", Z.MODE_PLAIN), ("tc_fp16", Z.MODE_TC_FP16)):
+        for form, mode in (("plain", Z.MODE_PLAIN), ("fast", Z.MODE_FAST), ("tc_fp16", Z.MODE_TC_FP16)):
             res = {}
             for o in self.orders:
                 p = Z.Plan(Z.C2C, o, np.float32, mode=mode, device=self.A.device.index)
@@ -352,6 +364,8 @@ class Cfft2G:
                 res[f"order{o}"] = {"gbs": round(2 * 16 * self.total / (ms / 1e3) / 1e9, 1),
                                     "max_rel_l2": float(err.max()), "tolerance": 4 * o * 2.0 ** -24}
             out[form] = res
+        if self.tuning is not None:
+            out["autotuned_plans"] = self.tuning
         return out
 
     batch = 1 << 14  # largest per-order batch (order 14), for sample sizing
@@ -582,7 +596,10 @@ class Cfft64:
         import zldsp_fft_b200 as Z
         self.Z = Z
         n = 1 << self.order
-        self.plan = Z.Plan(Z.C2C, self.order, np.float64, device=device)
+        Z.autotune(Z.C2C, self.order, self.order, np.float64, device=device)  # set-up: per-order plan choice
+        self.tuning = Z.tuning(Z.C2C, self.order, np.float64, device=device)
+        self.form = "tuned"
+        self.plan = Z.Plan(Z.C2C, self.order, np.float64, mode=Z.MODE_TUNED, device=device)
         g = torch.Generator(device=device)
         g.manual_seed(1005)
         self.A = (torch.rand((self.batch, n, 2), generator=g, device=device, dtype=torch.float64) * 2 - 1)
@@ -605,7 +622,8 @@ class Cfft64:
         import torch
         Z = self.Z
         n, b = 1 << self.order, self.batch
-        p32 = Z.Plan(Z.C2C, self.order, np.float32, device=self.A.device.index)
+        Z.autotune(Z.C2C, self.order, self.order, np.float32, device=self.A.device.index)
+        p32 = Z.Plan(Z.C2C, self.order, np.float32, mode=Z.MODE_TUNED, device=self.A.device.index)
         a32 = self.A.float()
         b32 = torch.empty_like(a32)
         c32 = torch.empty_like(a32)
@@ -632,6 +650,7 @@ class Cfft64:
         ref = np.fft.fft(x, axis=-1)
         nrm = np.linalg.norm(ref, axis=-1)
         return {
+            "autotuned_plan": self.tuning,
             "cfft_float_same_shape": {"gbs": round(f32_bytes / (ms32 / 1e3) / 1e9, 1), "ms_per_step": round(ms32, 4),
                                       "transforms_per_s": round(2 * b / (ms32 / 1e3))},
             "max_rel_l2_vs_numpy_fp64": {"f64": float((np.linalg.norm(y64 - ref, axis=-1) / nrm).max()),
@@ -1066,9 +1085,7 @@ def run_ours(args, wl_cls):
         "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic",
         "config": {"workload": wl.desc,
-                   "form": ("tensor-core split FP16 hi/lo, FP32 accumulate (256-point passes), plain FP32 elsewhere"
-                            if getattr(wl, "form", "plain") == "tc" else
-                            "plain FP32 (reference's Stockham radix-4/8 DIT, CUDA cores)"),
+                   "form": FORMS.get(getattr(wl, "form", "plain"), FORMS["plain"]),
                    "l2": getattr(wl, "l2", "rotating input/output sets, each step > 2x L2 (no L2 flush needed)"),
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -1106,14 +1123,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-autotune", action="store_true",
                     help="mixed only: skip the per-order autotuning in set-up (for profiling runs)")
-    ap.add_argument("--form", choices=["plain", "tc"], default="plain",
-                    help="cfft2g only: the plain FP32 form or the tensor-core split FP16 hi/lo form")
+    ap.add_argument("--form", choices=["tuned", "plain", "fast", "tc"], default="tuned",
+                    help="cfft2g only: the autotuned form per order (default), the plain form (the reference's "
+                         "arithmetic), the fast-twiddle form, or the tensor-core split FP16 hi/lo form")
     ap.add_argument("--total-log2", type=int, default=None,
                     help="cfft2g only: complex elements per order = 2^k (default 28 = 2 GiB); smaller cases "
                          "are for profiling and are not the benchmark configuration")
     args = ap.parse_args()
     wl_cls = WORKLOADS[args.workload]
-    if args.workload == "cfft2g" and (args.total_log2 is not None or args.form != "plain"):
+    if args.workload == "cfft2g" and (args.total_log2 is not None or args.form != "tuned"):
         base = wl_cls
         tl = args.total_log2 if args.total_log2 is not None else 28
         wl_cls = lambda: base(total_log2=tl, form=args.form)  # noqa: E731
