@@ -113,3 +113,28 @@ def test_fast_twiddle_form_within_tolerance(oracle, prec, ft, ct, order):
     back = G.run_c2r(rf, X.astype(ct))
     assert oracle.rel_l2(back, oracle.rfft_backward_fp64(X.astype(ct))).max() <= tol
     assert fast.device_status() == 0 and rf.device_status() == 0
+
+
+@pytest.mark.parametrize("order", [11, 12, 13])
+def test_fast_twiddle_form_tile_orders(oracle, order):
+    """The fast-twiddle form of the single-tile kernels' middle radix-16 groups
+    (CFFT orders 11-13, RFFT orders 12-14): within the FP32 bar, and not the
+    plain form's bits."""
+    from tests import gpu_util as G
+    rng = np.random.default_rng(800 + order)
+    n = 1 << order
+    x = (rng.uniform(-1, 1, (20, n)) + 1j * rng.uniform(-1, 1, (20, n))).astype(np.complex64)
+    tol = oracle.tolerance(order, "f32")
+    fast = Z.Plan(Z.C2C, order, np.float32, mode=Z.MODE_FAST)
+    y = G.run_c2c(fast, x, True)
+    assert oracle.rel_l2(y, oracle.cfft_fp64(x)).max() <= tol
+    assert not np.array_equal(y, G.run_c2c(Z.Plan(Z.C2C, order, np.float32), x, True))
+    assert oracle.rel_l2(G.run_c2c(fast, y, False), oracle.cfft_fp64(y, False)).max() <= tol
+    xr = rng.uniform(-1, 1, (20, 2 * n)).astype(np.float32)
+    rf = Z.Plan(Z.R2C, order + 1, np.float32, mode=Z.MODE_FAST)
+    rtol = oracle.tolerance(order + 1, "f32")
+    for ol in (Z.AOS, Z.SOA):
+        X = G.run_r2c(rf, xr, ol)
+        assert oracle.rel_l2(X, oracle.rfft_fp64(xr)).max() <= rtol
+    Pw = G.run_r2c(rf, xr, sqr_mag=True)
+    assert oracle.rel_l2(Pw, np.abs(oracle.rfft_fp64(xr)) ** 2).max() <= 2 * rtol

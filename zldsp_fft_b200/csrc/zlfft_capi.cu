@@ -649,6 +649,7 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     }
     const zlfft::TileTable& t = p->prec == ZLFFT_F32 ? tables().f32 : tables().f64;
     zlfft::TileLaunchFn fn = t.fn[P][dop][in_layout][out_layout];
+    if (p->fast_form && in_layout == ZLFFT_AOS && t.fast[P][dop][out_layout]) fn = t.fast[P][dop][out_layout];
     if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no kernel for this configuration");
     DeviceGuard g(p->device);
     cudaError_t e = fn(a, stream, ctx);
@@ -1766,12 +1767,16 @@ int autotune_impl(int device, int kind, int prec, size_t lo, size_t hi) {
                                 }
             }
         } else {
-            for (int tma : {1, 0}) {
-                TuneEntry c;
-                c.chunk_mb = 0;
-                c.streams = 1;
-                c.tma = tma;
-                cands.push_back(c);
+            for (int form : {ZLFFT_MODE_PLAIN, ZLFFT_MODE_FAST}) {
+                if (form == ZLFFT_MODE_FAST && cfft_order < 11) continue;  // no middle radix-16 group
+                for (int tma : {1, 0}) {
+                    TuneEntry c;
+                    c.chunk_mb = 0;
+                    c.streams = 1;
+                    c.tma = tma;
+                    c.form = form;
+                    cands.push_back(c);
+                }
             }
         }
         TuneEntry best;

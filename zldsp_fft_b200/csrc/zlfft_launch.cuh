@@ -33,12 +33,15 @@ struct TileTable {
     // STFT front end: RFFT forward with the window multiplied in at load,
     // [order][0: forward, 1: forward_sqr_mag][out_layout]
     TileLaunchFn stft[kTileMaxP + 1][2][2];
+    // fast-twiddle form of the orders with middle radix-16 groups (11..13),
+    // AoS input: [order][op][out_layout]
+    TileLaunchFn fast[kTileMaxP + 1][5][2];
 };
 
-template <typename F, int P, int OP, int IL, int OL, bool WIN = false>
+template <typename F, int P, int OP, int IL, int OL, bool WIN = false, bool FAST = false>
 cudaError_t launch_tile(const TileArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = TileCfg<F, P, OP>;
-    auto kern = tile_kernel<F, P, OP, IL, OL, false, WIN>;
+    auto kern = tile_kernel<F, P, OP, IL, OL, false, WIN, FAST>;
     static const int blocks_per_sm = [kern]() {
         if (Cfg::SMEM > 48 * 1024) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
@@ -387,6 +390,10 @@ void fill_tile_c2c_order(TileTable& t) {
     t.fn[P][kC2CBwd][kAoS][kSoA] = launch_tile<F, P, kC2CBwd, kAoS, kSoA>;
     t.fn[P][kC2CBwd][kSoA][kAoS] = launch_tile<F, P, kC2CBwd, kSoA, kAoS>;
     t.fn[P][kC2CBwd][kSoA][kSoA] = launch_tile<F, P, kC2CBwd, kSoA, kSoA>;
+    if constexpr (P >= 11) {
+        t.fast[P][kC2CFwd][kAoS] = launch_tile<F, P, kC2CFwd, kAoS, kAoS, false, true>;
+        t.fast[P][kC2CBwd][kAoS] = launch_tile<F, P, kC2CBwd, kAoS, kAoS, false, true>;
+    }
 }
 
 // R2C/C2R: P is the inner CFFT order (real length 2^(P+1)). The real side has
@@ -405,6 +412,11 @@ void fill_tile_r2c_order(TileTable& t) {
     t.stft[P][0][kAoS] = launch_tile<F, P, kR2CFwd, kAoS, kAoS, true>;
     t.stft[P][0][kSoA] = launch_tile<F, P, kR2CFwd, kAoS, kSoA, true>;
     t.stft[P][1][kAoS] = t.stft[P][1][kSoA] = launch_tile<F, P, kR2CSqrMag, kAoS, kAoS, true>;
+    if constexpr (P >= 11) {
+        t.fast[P][kR2CFwd][kAoS] = launch_tile<F, P, kR2CFwd, kAoS, kAoS, false, true>;
+        t.fast[P][kR2CFwd][kSoA] = launch_tile<F, P, kR2CFwd, kAoS, kSoA, false, true>;
+        t.fast[P][kR2CSqrMag][kAoS] = t.fast[P][kR2CSqrMag][kSoA] = launch_tile<F, P, kR2CSqrMag, kAoS, kAoS, false, true>;
+    }
 }
 
 template <typename F, int... Ps>

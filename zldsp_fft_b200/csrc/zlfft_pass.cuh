@@ -135,44 +135,6 @@ struct PassMaps {
     CUtensorMap mo;  // first pass: the output, as rows of R points (one row per unit)
 };
 
-// Radix-16 group (not the first) of the fast-twiddle form, sub-length L,
-// in-group index k: the group equals a pre-twiddle of input register rho by
-// W_{16L}^{rho k} followed by the untwiddled radix-16 (stage A plain
-// radix-4s, stage B radix-4s with the constants W_16^{a m}), with the same
-// output order as group_compute. The 15 twiddles come from two table values,
-// W_{16L}^{k} and W_{16L}^{4k}, by products (at most four roundings), instead
-// of 15 table loads: results stay within the FP bar, but are not the
-// reference's bits.
-template <int P, int L, typename C>
-__device__ __forceinline__ void group16_fast(C* r, uint32_t k, const C* T) {
-    using F = decltype(C::x);
-    constexpr int s = P - ilog2c(16LL * L);  // W_{16L}^{j} = T[j << s], j < 4L < 3N/4 >> s
-    const C w1 = tw_load(T, k << s), w4 = tw_load(T, (4u * k) << s);
-    const C w2 = cmul_tw(w1, w1), w3 = cmul_tw(w1, w2);
-    const C w8 = cmul_tw(w4, w4), w12 = cmul_tw(w4, w8);
-    const C one = cx<C>((F)1, (F)0);
-    const C lo[4] = {one, w1, w2, w3};
-    const C hi[4] = {one, w4, w8, w12};
-#pragma unroll
-    for (int rho = 1; rho < 16; ++rho) {
-        const C w = (rho & 3) == 0 ? hi[rho >> 2] : ((rho >> 2) == 0 ? lo[rho & 3] : cmul_tw(lo[rho & 3], hi[rho >> 2]));
-        r[rho] = cmul_tw(r[rho], w);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) bfly4_first(r[a], r[a + 4], r[a + 8], r[a + 12]);
-    // W_16^j = exp(-2 pi i j / 16) for j = a * m
-    const C c1 = cx<C>((F)0.92387953251128674, (F)-0.38268343236508978);
-    const C c2 = cx<C>((F)0.70710678118654752, (F)-0.70710678118654752);
-    const C c3 = cx<C>((F)0.38268343236508978, (F)-0.92387953251128674);
-    const C c4 = cx<C>((F)0, (F)-1);
-    const C c6 = cx<C>((F)-0.70710678118654752, (F)-0.70710678118654752);
-    const C c9 = cx<C>((F)-0.92387953251128674, (F)0.38268343236508978);
-    bfly4_first(r[0], r[1], r[2], r[3]);
-    bfly4_tw(r[4], r[5], r[6], r[7], c1, c2, c3);
-    bfly4_tw(r[8], r[9], r[10], r[11], c2, c4, c6);
-    bfly4_tw(r[12], r[13], r[14], r[15], c3, c6, c9);
-}
-
 // Unit of slot u in work item ib of a last pass with the RFFT split fused:
 // the first half of the slots take units HALF*ib + u, the second half their
 // mirrors L_in - (HALF*ib + u) (unit L_in/2 stands in for the mirror of unit
