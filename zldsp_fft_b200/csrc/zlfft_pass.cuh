@@ -338,9 +338,10 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                                 __syncthreads();
                                 if (threadIdx.x == 0) {
                                     const int y = (int)(tr * Cfg::UNITS + (U - u));
+                                    const uint64_t pol = l2_policy_evict_last();  // the next pass reads it from L2
 #pragma unroll 1
                                     for (int bx = 0; bx < R / CPB; ++bx)
-                                        tma_store_2d(&maps.mo, bx * CPB * 2, y, smem + (size_t)bx * UPC * 128);
+                                        tma_store_2d_hint(&maps.mo, bx * CPB * 2, y, smem + (size_t)bx * UPC * 128, pol);
                                     bulk_commit();
                                 }
                                 return;
