@@ -98,7 +98,13 @@ struct PassCfg {
                                       (size_t)UPC * R * sizeof(C) <= XBYTES;
     static constexpr int UNITS = N / R;            // units per transform
     static constexpr int CPT = UNITS / UPC;        // CTAs (work items) per transform
-    static constexpr int MINB = (65536 / (THREADS * 96)) > 0 ? (65536 / (THREADS * 96)) : 1;
+    // Resident CTAs per SM: as many as the shared memory allows, within a
+    // budget of 80 registers per thread in FP32 and 96 in FP64 (a cap of ~100
+    // made the FP64 plain form spill).
+    static constexpr int SMEM_CTAS = (227 * 1024) / (int)(SMEM + 1024);
+    static constexpr int REG_CTAS = 65536 / (THREADS * (sizeof(F) == 4 ? 80 : 96));
+    static constexpr int MINB_ = SMEM_CTAS < REG_CTAS ? SMEM_CTAS : REG_CTAS;
+    static constexpr int MINB = MINB_ > 0 ? MINB_ : 1;
     static_assert(UNITS % UPC == 0, "a transform must split into whole CTAs");
     static_assert(SMEM <= 200 * 1024, "pass tile too large");
 };
@@ -217,6 +223,28 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
     }
     uint32_t phase = 0;
 
+    // Fast form: the two table twiddles of each radix-16 group (a thread runs
+    // one butterfly per such group: E == 16), loaded at the item's start,
+    // ahead of the input wait.
+    [[maybe_unused]] C fw[GE - GB][2];
+    auto load_fw = [&](int ku) {
+        if constexpr (FAST) {
+            [&]<int... GI>(std::integer_sequence<int, GI...>) {
+                (
+                    [&] {
+                        constexpr Grp G = tile_group(P, GB + GI);
+                        if constexpr (G.R == 16 && !G.first) {
+                            static_assert(G.R == E, "one radix-16 butterfly per thread");
+                            constexpr int ELL = G.L / L_IN;
+                            const uint32_t kk = (uint32_t)(ku + L_IN * (tb % ELL));
+                            group16_fast_tw<P, G.L>(kk, static_cast<const C*>(a.tw), fw[GI][0], fw[GI][1]);
+                        }
+                    }(),
+                    ...);
+            }(std::make_integer_sequence<int, GE - GB>{});
+        }
+    };
+
     for (long long item = blockIdx.x; item < items; item += gridDim.x) {
         // the previous item's output stores have read the exchange buffer before
         // anyone writes it again (the first write follows a barrier)
@@ -226,6 +254,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
         const int U = SPLIT ? split_unit<L_IN, UPC>(ib, u) : ib * UPC + u;
         const int ku = U % L_IN;  // k of the unit
         const int J = U / L_IN;
+        load_fw(ku);
         C v[E];
         if constexpr (Cfg::kTMA) {
             if (use_tma) {
@@ -295,7 +324,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                         const int b = tb + i * T;
                         const uint32_t kk = (uint32_t)(ku + L_IN * (b % ELL));
                         if constexpr (FAST && G.R == 16 && !G.first) {
-                            group16_fast<P, G.L>(v + i * G.R, kk, static_cast<const C*>(a.tw));
+                            group16_fast_w(v + i * G.R, fw[GI][0], fw[GI][1]);
                         } else {
                             group_compute_ld<P, G.R, G.L, G.first>(v + i * G.R, kk, tws);
                         }
