@@ -4,10 +4,17 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
 Workloads (synthetic, seeded; shapes from the reference benchmark configs):
+  cfft2g      (default) CFFT<float> orders 14/16/20, 2 GiB each, forward +
+              backward, autotuned plans; per-order plain / fast / TC comparison.
   rfft12      RFFT<float> order 12 (N = 4096), 8192 Hann-windowed frames of
               3 sinusoids + N(0, 0.1^2) noise; one step = forward to AoS,
               forward to split SoA and forward_sqr_mag over the whole batch
               (plain FP32 CUDA-core form).
+  cfft10      one CFFT<float> order-10 transform, forward + backward (latency).
+  mixed       20,000 transforms of orders 6..16, CFFT and RFFT, one graph.
+  cfft64      CFFT<double> order 16 x 512, forward + backward.
+  stft        fused STFT front end (framing, Hann window, forward_sqr_mag).
+  istft       fused inverse STFT (filter, RFFT backward, window, overlap-add).
 
 Metric: algorithmic HBM bytes (one read of each input, one write of each
 output; twiddles excluded) per second, in GB/s; roofline = the measured HBM
@@ -46,6 +53,51 @@ FORMS = {
 
 
 # ------------------------------------------------------------------ helpers
+def pcie_probe(nbytes=256 << 20, reps=5):
+    """Pinned-memory copy rates of this box (GB/s): host->device, device->host,
+    and both at once on two streams. They bound the host-API (e2e) figure."""
+    import torch
+    h1 = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    h2 = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d1 = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d2 = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def h2d():
+        with torch.cuda.stream(s1):
+            d1.copy_(h1, non_blocking=True)
+
+    def d2h():
+        with torch.cuda.stream(s2):
+            h2.copy_(d2, non_blocking=True)
+
+    def both():
+        h2d()
+        d2h()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    th, td, tb = timed(h2d), timed(d2h), timed(both)
+    del h1, h2, d1, d2
+    return {"h2d": round(nbytes / th / 1e9, 2), "d2h": round(nbytes / td / 1e9, 2),
+            "both_directions": round(2 * nbytes / tb / 1e9, 2)}
+
+
+def e2e_bound(bytes_per_step, h2d_bytes, d2h_bytes, pcie):
+    """Highest e2e GB/s the copies allow: the step takes at least the longest of
+    its H2D copy, its D2H copy, and both sharing the link."""
+    t = max(h2d_bytes / (pcie["h2d"] * 1e9), d2h_bytes / (pcie["d2h"] * 1e9),
+            (h2d_bytes + d2h_bytes) / (pcie["both_directions"] * 1e9))
+    return bytes_per_step / t / 1e9 if t > 0 else None
+
+
 def measured_hbm_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -937,7 +989,158 @@ class Stft:
         return float(4 * ((frames - 1) * hop + n) + 4 * self.nb * frames), dt
 
 
-WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G, "mixed": Mixed, "cfft64": Cfft64, "cfft10": Cfft10, "stft": Stft}
+class Istft:
+    """Inverse STFT / overlap-add: the bins of 131,069 frames of 4096 points
+    (the stft workload's shape; complex U[-1, 1), seed 1007, real DC and
+    Nyquist bins), times a spectral filter (a delayed low-pass), RFFT backward,
+    periodic Hann synthesis window, and overlap-add at hop 1024 into a
+    2^27-sample signal, in one zlfft_istft_device launch. Algorithmic bytes:
+    the bins read once plus the signal written. Beside it: the same synthesis
+    unfused (torch filter multiply, the batched RFFT backward into a frames
+    buffer, torch window multiply and strided overlap-add)."""
+    name = "istft"
+    desc = ("inverse STFT: 131,069 frames of 4096-point bins (complex64 AoS), spectral filter, RFFT backward, "
+            "Hann synthesis window, overlap-add at hop 1024 into a 2^27-sample signal, fused")
+    l2 = "each step reads 2.15 GB and writes 512 MiB, > 20x L2 (no L2 flush needed)"
+    order, hop, total = 12, 1024, 1 << 27
+    dtype = "f32"
+
+    def __init__(self):
+        n = 1 << self.order
+        self.frame_n = n
+        self.nf = (self.total - n) // self.hop + 1
+        self.nb = n // 2 + 1
+        self.op_bytes = {"istft_filter_window": 8 * self.nb * self.nf + 4 * self.total}
+        self.bytes_per_step = self.op_bytes["istft_filter_window"]
+        self.dominant = "istft_filter_window"
+        self.batch = self.nf
+        self.host_in = None
+
+    @staticmethod
+    def filter_bins(nb, n, xp, dtype):
+        """H[k] = exp(-2 pi i 64 k / n) / (1 + (k / 256)^2): a 64-sample delay and a low-pass."""
+        k = xp.arange(nb, dtype=dtype)
+        mag = 1.0 / (1.0 + (k / 256.0) ** 2)
+        ph = -2.0 * np.pi * 64.0 * k / n
+        return mag * xp.cos(ph), mag * xp.sin(ph)
+
+    def setup(self, device):
+        import torch
+        import zldsp_fft_b200 as Z
+        self.Z = Z
+        g = torch.Generator(device=device)
+        g.manual_seed(1007)
+        self.bins = (torch.rand((self.nf, self.nb, 2), generator=g, device=device) * 2 - 1).contiguous()
+        self.bins[:, 0, 1] = 0
+        self.bins[:, -1, 1] = 0
+        t = torch.arange(self.frame_n, dtype=torch.float64, device=device)
+        self.win = (0.5 - 0.5 * torch.cos(2 * np.pi * t / self.frame_n)).float().contiguous()
+        hr, hi = self.filter_bins(self.nb, self.frame_n, torch, torch.float64)
+        self.filt = torch.stack([hr, hi], -1).to(device).float().contiguous()
+        self.sig = torch.empty(self.total, dtype=torch.float32, device=device)
+        self.plan = Z.Plan(Z.R2C, self.order, np.float32, device=device)
+        torch.cuda.synchronize(device)
+
+    def ops(self, step):
+        Z = self.Z
+
+        def run(st):
+            self.plan.istft(Z.AOS, self.bins.data_ptr(), None, self.hop, self.nf, self.sig.data_ptr(),
+                            filter=self.filt.data_ptr(), window=self.win.data_ptr(), stream=st)
+        return [("istft_filter_window", run)]
+
+    def take_launches(self):
+        return self.plan.take_launch_count()
+
+    def compare(self, stream, reps):
+        """The unfused path and its relative L2 distance from the fused result
+        (the unfused overlap-add sums the frames in another order)."""
+        import torch
+        Z = self.Z
+        n, hop, nf = self.frame_n, self.hop, self.nf
+        k = n // hop
+        frames = torch.empty((nf, n), dtype=torch.float32, device=self.bins.device)
+        ref = torch.empty_like(self.sig)
+        b = torch.view_as_complex(self.bins)
+        h = torch.view_as_complex(self.filt)
+
+        def unfused():
+            with torch.cuda.stream(stream):
+                fb = torch.view_as_real(b * h).contiguous()
+                self.plan.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, fb.data_ptr(), None, frames.data_ptr(), None, nf,
+                                      stream=stream.cuda_stream)
+                fw = frames * self.win
+                ref.zero_()
+                for r in range(k):  # frames r, r + K, ... tile the signal from r * hop without overlap
+                    cnt = (nf - r + k - 1) // k
+                    ref[r * hop:r * hop + cnt * n] += fw[r::k].reshape(-1)
+        for _ in range(2):
+            unfused()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            unfused()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        self.ops(0)[0][1](stream.cuda_stream)
+        torch.cuda.synchronize()
+        d = (torch.linalg.vector_norm((self.sig - ref).double()) / torch.linalg.vector_norm(ref.double())).item()
+        return {"unfused_filter_rfft_window_overlap_add": {"gbs": round(self.bytes_per_step / (ms / 1e3) / 1e9, 1),
+                                                           "ms": round(ms, 3)},
+                "fused_vs_unfused_rel_l2": d}
+
+    def cpu_sample_desc(self, frames):
+        return (f"{frames} of {self.nf} frames: numpy filter multiply, the reference's RFFT backward, numpy window "
+                f"and sequential overlap-add, median of 3")
+
+    def setup_e2e(self):
+        import torch
+        self.h_bins = self.bins.cpu().pin_memory()
+        self.h_sig = torch.empty(self.total, dtype=torch.float32).pin_memory()
+        self.e2e_h2d = self.h_bins.numel() * 4
+        self.e2e_d2h = self.h_sig.numel() * 4
+
+    def e2e_step(self):
+        import torch
+        st = torch.cuda.current_stream()
+        self.bins.copy_(self.h_bins, non_blocking=True)
+        self.ops(0)[0][1](st.cuda_stream)
+        self.h_sig.copy_(self.sig, non_blocking=True)
+        st.synchronize()
+
+    def cpu_run(self, frames, threads, kind):
+        from oracle import oracle as O
+        n, hop = self.frame_n, self.hop
+        frames = max(1, min(frames, self.nf))
+        rng = np.random.default_rng(1007)
+        X = (rng.uniform(-1, 1, (frames, self.nb)) + 1j * rng.uniform(-1, 1, (frames, self.nb))).astype(np.complex64)
+        X[:, 0], X[:, -1] = X[:, 0].real, X[:, -1].real
+        hr, hi = self.filter_bins(self.nb, n, np, np.float64)
+        H = (hr + 1j * hi).astype(np.complex64)
+        win = (0.5 - 0.5 * np.cos(2 * np.pi * np.arange(n) / n)).astype(np.float32)
+        if kind == "reference":
+            plan = O.RefPlan("r2c", self.order, "f32", threads)
+            t0 = time.perf_counter()
+            Y = np.empty_like(X)
+            Y.real = X.real * H.real - X.imag * H.imag
+            Y.imag = X.real * H.imag + X.imag * H.real
+            x = plan.rfft_backward(Y) * win
+            y = np.zeros((frames - 1) * hop + n, np.float32)
+            for f in range(frames):
+                y[f * hop:f * hop + n] += x[f]
+            dt = time.perf_counter() - t0
+            plan.close()
+        else:
+            t0 = time.perf_counter()
+            O.istft_port(X, hop, H, win)
+            dt = time.perf_counter() - t0
+        return float(8 * self.nb * frames + 4 * ((frames - 1) * hop + n)), dt
+
+
+WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G, "mixed": Mixed, "cfft64": Cfft64, "cfft10": Cfft10, "stft": Stft,
+             "istft": Istft}
 
 
 # ------------------------------------------------------------------ CPU baseline
@@ -1074,6 +1277,8 @@ def run_ours(args, wl_cls):
     e2e_s = replicas.max_over_ranks(e2e_s, dist, device="cuda")
     e2e_val = replicas.aggregate_gbs(wl.bytes_per_step * e2e_steps, world, e2e_s)
     wl.take_launches()
+    pcie = pcie_probe()
+    bound = e2e_bound(wl.bytes_per_step, wl.e2e_h2d, wl.e2e_d2h, pcie)
     schedules = wl.compare(stream, max(3, min(args.steps, 10))) if hasattr(wl, "compare") else None
 
     peak, peak_kind = measured_hbm_peak()
@@ -1095,7 +1300,9 @@ def run_ours(args, wl_cls):
         "per_op_gbs": {k: round(wl.op_bytes[k] / (v / 1e3) / 1e9, 1) for k, v in per_op_ms.items()},
         "per_op_us": {k: round(v * 1e3, 2) for k, v in per_op_ms.items()},
         "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": wl.e2e_h2d,
-                "d2h_bytes_per_step": wl.e2e_d2h, "api": "zlfft_exec_host_batched, pinned host buffers"},
+                "d2h_bytes_per_step": wl.e2e_d2h, "api": "zlfft_exec_host_batched, pinned host buffers",
+                "pcie_gbs": pcie, "pcie_bound": round(bound, 2) if bound else None,
+                "frac_of_pcie_bound": round(e2e_val / bound, 3) if bound else None},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }

@@ -137,6 +137,24 @@ ZLFFT_API int zlfft_stft_device(zlfft_plan plan, int op, int out_layout, const v
                                 const void* window, void* out0, void* out1, size_t n_frames, size_t out_stride,
                                 void* stream);
 
+/* Inverse STFT with overlap-add on DEVICE buffers, the backward-side fusion of
+ * the STFT: frame f's bins (N/2+1 complex, AoS in0 or SoA in0/in1, frame f at
+ * + f*in_stride, 0 = dense) are multiplied by filter[k] (N/2+1 complex;
+ * NULL = none; each complex product rounded operation by operation), go
+ * through RFFT::backward (src/zldsp_fft_rfft.hpp:86-100; unnormalised), are
+ * multiplied by window[n] (N reals; NULL = none) and added into
+ * signal[f*hop + n]. The signal ((n_frames - 1) * hop + N reals) is written,
+ * not accumulated into: each real is the sum of its frames' terms in
+ * ascending frame order starting from zero, one rounding per term, so the
+ * result is that of a sequential loop over frames, bit for bit. hop must be
+ * even and divide N. Frame orders 10-14 (FP32) or 10-13 (FP64). With the
+ * bins of a zero-padded signal and a filter's spectrum this is overlap-add
+ * fast convolution. No reference counterpart: the reference offers the
+ * per-frame RFFT::backward only. */
+ZLFFT_API int zlfft_istft_device(zlfft_plan plan, int in_layout, const void* in0, const void* in1, size_t in_stride,
+                                 const void* filter, const void* window, size_t hop, size_t n_frames, void* signal,
+                                 void* stream);
+
 /* As zlfft_exec_device, for callers that cannot allocate device memory when
  * they run a transform: a real-time audio thread (an allocation can block
  * for an unbounded time), work being captured into a CUDA graph (cudaMalloc

@@ -174,6 +174,46 @@ def rfft_backward_port(X: np.ndarray) -> np.ndarray:
     return out
 
 
+def istft_port(X: np.ndarray, hop: int, filt=None, win=None) -> np.ndarray:
+    """Inverse STFT with overlap-add, sequentially: bins X (frames, N/2+1) ->
+    signal of (frames - 1) * hop + N reals, y[f*hop + n] += win[n] * x_f[n] for
+    f = 0, 1, ... in order, x_f = RFFT backward (the port) of filt * X_f. Every
+    product and sum is one operation in the bins' precision (numpy array
+    arithmetic, so no fused multiply-adds)."""
+    X = np.ascontiguousarray(X)
+    ft = np.float32 if X.dtype == np.complex64 else np.float64
+    if filt is not None:
+        xr, xi = X.real.astype(ft), X.imag.astype(ft)
+        hr, hi = filt.real.astype(ft), filt.imag.astype(ft)
+        Y = np.empty_like(X)
+        Y.real = xr * hr - xi * hi
+        Y.imag = xr * hi + xi * hr
+        X = Y
+    x = rfft_backward_port(X)
+    frames, n = x.shape
+    if win is not None:
+        x = x * np.asarray(win, ft)[None, :]
+    y = np.zeros((frames - 1) * hop + n, ft)
+    for f in range(frames):
+        y[f * hop:f * hop + n] += x[f]
+    return y
+
+
+def istft_fp64(X: np.ndarray, hop: int, filt=None, win=None) -> np.ndarray:
+    """The same overlap-add in float64 from numpy.fft (RFFT backward = (N/2) irfft)."""
+    X = np.asarray(X, np.complex128)
+    if filt is not None:
+        X = X * np.asarray(filt, np.complex128)[None, :]
+    x = rfft_backward_fp64(X)
+    frames, n = x.shape
+    if win is not None:
+        x = x * np.asarray(win, np.float64)[None, :]
+    y = np.zeros((frames - 1) * hop + n)
+    for f in range(frames):
+        y[f * hop:f * hop + n] += x[f]
+    return y
+
+
 # ----------------------------------------------------------------- reference (shim-built)
 class RefPlan:
     """One reference CFFT/RFFT instance per thread (the reference is single-threaded)."""

@@ -143,3 +143,22 @@ def test_twiddle_table_matches_reference_formula(oracle):
             T = oracle.twiddles(order, prec)
             expect = (np.cos(a * np.pi) + 1j * np.sin(a * np.pi)).astype(ct)
             assert np.array_equal(T, expect)
+
+
+def test_istft_port_overlap_add(oracle):
+    """The sequential inverse STFT: hop = N concatenates the frames' RFFT
+    backward outputs; overlapping hops stay within the FP64 oracle's bar."""
+    rng = np.random.default_rng(1501)
+    order, nf = 9, 6
+    n = 1 << order
+    X = (rng.uniform(-1, 1, (nf, n // 2 + 1)) + 1j * rng.uniform(-1, 1, (nf, n // 2 + 1))).astype(np.complex64)
+    X[:, 0], X[:, -1] = X[:, 0].real, X[:, -1].real
+    y = oracle.istft_port(X, n)
+    assert np.array_equal(y, oracle.rfft_backward_port(X).reshape(-1))
+    win = (0.5 - 0.5 * np.cos(2 * np.pi * np.arange(n) / n)).astype(np.float32)
+    H = X[0]
+    for hop in (n // 2, n // 4, 2):
+        y = oracle.istft_port(X, hop, H, win)
+        ref = oracle.istft_fp64(X, hop, H, win)
+        assert y.shape == ((nf - 1) * hop + n,)
+        assert np.linalg.norm(y - ref) / np.linalg.norm(ref) <= (n // hop) * oracle.tolerance(order, "f32")

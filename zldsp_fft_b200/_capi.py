@@ -54,6 +54,7 @@ EXPORTS = (
     "zlfft_exec_device",
     "zlfft_exec_device_noalloc",
     "zlfft_stft_device",
+    "zlfft_istft_device",
     "zlfft_plan_take_launch_count",
     "zlfft_plan_copy_twiddles",
     "zlfft_plan_device_status",
@@ -107,6 +108,7 @@ def lib() -> ctypes.CDLL:
         L.zlfft_exec_device.argtypes = [vp, i, i, i, vp, vp, vp, vp, sz, sz, sz, vp]
         L.zlfft_exec_device_noalloc.argtypes = [vp, i, i, i, vp, vp, vp, vp, sz, sz, sz, vp]
         L.zlfft_stft_device.argtypes = [vp, i, i, vp, sz, vp, vp, vp, sz, sz, vp]
+        L.zlfft_istft_device.argtypes = [vp, i, vp, vp, sz, vp, vp, sz, sz, vp, vp]
         L.zlfft_plan_take_launch_count.argtypes = [vp, ctypes.POINTER(sz)]
         L.zlfft_plan_copy_twiddles.argtypes = [vp, vp, sz, ctypes.POINTER(sz)]
         L.zlfft_plan_device_status.argtypes = [vp, ctypes.POINTER(i)]

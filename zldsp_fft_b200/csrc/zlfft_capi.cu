@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/zlfft.h"
+#include "zlfft_istft.cuh"
 #include "zlfft_launch.cuh"
 #include "zlfft_mixed.cuh"
 
@@ -142,7 +143,11 @@ struct TablesHolder {
     zlfft::GatherTable g32{};
     zlfft::GatherTable g64{};
     zlfft::TcPassTable tc{};
+    zlfft::IstftTable i32{};
+    zlfft::IstftTable i64{};
     TablesHolder() {
+        zlfft::fill_istft_f32(i32);
+        zlfft::fill_istft_f64(i64);
         zlfft::fill_tc_pass_a(tc);
         zlfft::fill_tc_pass_b(tc);
         zlfft::fill_gather_f32(g32);
@@ -705,6 +710,55 @@ int stft_impl(zlfft_plan_s* p, int op, int out_layout, const void* signal, size_
     DeviceGuard g(p->device);
     cudaError_t e = fn(a, stream, ctx);
     if (e != cudaSuccess) return cuda_fail(e, "STFT launch");
+    return ZLFFT_OK;
+}
+
+// Inverse STFT / overlap-add (zlfft_istft.cuh): validation and dispatch.
+int istft_impl(zlfft_plan_s* p, int in_layout, const void* in0, const void* in1, size_t in_stride, const void* filter,
+               const void* window, size_t hop, size_t n_frames, void* signal, cudaStream_t stream) {
+    if (p->kind != ZLFFT_R2C) return fail(ZLFFT_ERR_INVALID_ARG, "the inverse STFT needs an RFFT plan");
+    if (in_layout != ZLFFT_AOS && in_layout != ZLFFT_SOA) return fail(ZLFFT_ERR_INVALID_ARG, "invalid layout");
+    const zlfft::IstftTable& t = p->prec == ZLFFT_F32 ? tables().i32 : tables().i64;
+    const int pc = p->cfft_order;
+    zlfft::IstftLaunchFn fn = (pc >= 0 && pc <= zlfft::kTileMaxP) ? t.fn[pc][in_layout] : nullptr;
+    if (!fn)
+        return fail(ZLFFT_ERR_UNSUPPORTED, "inverse STFT frame orders are 10-%d for this precision",
+                    p->prec == ZLFFT_F32 ? 14 : 13);
+    const size_t n = size_t{1} << p->order;  // frame length in reals
+    if (hop == 0 || hop % 2 || n % hop) return fail(ZLFFT_ERR_INVALID_ARG, "hop must be even and divide the frame length");
+    const bool soa = in_layout == ZLFFT_SOA;
+    if (!in0 || (soa && !in1) || !signal) return fail(ZLFFT_ERR_INVALID_ARG, "null buffer pointer");
+    const size_t pair = 2 * p->esize;
+    if (!aligned(in0, soa ? p->esize : pair) || (soa && !aligned(in1, p->esize)))
+        return fail(ZLFFT_ERR_ALIGNMENT, "bins must be aligned to their element type");
+    if ((filter && !aligned(filter, pair)) || (window && !aligned(window, pair)) || !aligned(signal, pair))
+        return fail(ZLFFT_ERR_ALIGNMENT, "filter, window and signal must be %zu-byte aligned", pair);
+    const size_t nb = n / 2 + 1;
+    if (in_stride == 0) in_stride = nb;
+    if (n_frames > 1 && in_stride < nb) return fail(ZLFFT_ERR_INVALID_ARG, "input stride smaller than one frame");
+    if (n_frames == 0) return ZLFFT_OK;
+    zlfft::TileArgs a{};
+    a.in0 = in0;
+    a.in1 = soa ? in1 : nullptr;
+    a.batch = (long long)n_frames;
+    a.in_stride = (long long)in_stride;
+    a.out_stride = 0;
+    a.tw = p->d_tw;
+    a.tws = p->d_tws;
+    a.rw = p->d_rw;
+    a.err = p->d_err;
+    zlfft::IstftArgs o{};
+    o.filt = filter;
+    o.win = window;
+    o.sig = signal;
+    o.n_frames = (long long)n_frames;
+    o.hop = (long long)hop;
+    o.k = (int)(n / hop);
+    o.blocks = (long long)n_frames + o.k - 1;
+    zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
+    DeviceGuard g(p->device);
+    cudaError_t e = fn(a, o, stream, ctx);
+    if (e != cudaSuccess) return cuda_fail(e, "inverse STFT launch");
     return ZLFFT_OK;
 }
 
@@ -1533,6 +1587,13 @@ int zlfft_stft_device(zlfft_plan plan, int op, int out_layout, const void* signa
     if (!plan) return fail(ZLFFT_ERR_INVALID_ARG, "null plan");
     return stft_impl(plan, op, out_layout, signal, hop, window, out0, out1, n_frames, out_stride,
                      static_cast<cudaStream_t>(stream));
+}
+
+int zlfft_istft_device(zlfft_plan plan, int in_layout, const void* in0, const void* in1, size_t in_stride,
+                       const void* filter, const void* window, size_t hop, size_t n_frames, void* signal, void* stream) {
+    if (!plan) return fail(ZLFFT_ERR_INVALID_ARG, "null plan");
+    return istft_impl(plan, in_layout, in0, in1, in_stride, filter, window, hop, n_frames, signal,
+                      static_cast<cudaStream_t>(stream));
 }
 
 int zlfft_exec_device_noalloc(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0,

@@ -132,6 +132,23 @@ struct TileArgs {
     const void* win;
 };
 
+// Output sink of the backward RFFT's last group. NoSink: the transform's
+// samples go to the output array. A sink with kActive (the overlap-add of
+// zlfft_istft.cuh) receives them instead, as add(pos, x) with x = real samples
+// 2 pos and 2 pos + 1, and may carry a spectral filter h (N + 1 bins,
+// multiplied into the bins as the pre-step reads them; null: none).
+struct NoSink {
+    static constexpr bool kActive = false;
+    const void* h = nullptr;
+};
+
+// Complex product with each operation rounded on its own:
+// (x.re h.re - x.im h.im, x.re h.im + x.im h.re).
+template <typename C>
+__device__ __forceinline__ C cmul_rn(const C x, const C h) {
+    return cx<C>(sub_rn(mul_rn(x.x, h.x), mul_rn(x.y, h.y)), add_rn(mul_rn(x.x, h.y), mul_rn(x.y, h.x)));
+}
+
 template <typename F, int P, int OP = kC2CFwd, int BLOCK = 128>
 struct TileCfg {
     using C = Cx<F>;
@@ -494,9 +511,12 @@ struct TileWorker {
 
     // Process tile `tile`. With use_tma, group 0 reads this tile's input from
     // the staging buffer that follows the exchange buffer in shared memory
-    // (placed there by TMA) and calls refill() once done.
-    template <class Refill>
-    __device__ __forceinline__ void run(const TileArgs& a, long long tile, bool use_tma, Refill&& refill) {
+    // (placed there by TMA) and calls refill() once done. A backward RFFT may
+    // hand its output samples to `sink` (see NoSink).
+    template <class Refill, class Sink = NoSink>
+    __device__ __forceinline__ void run(const TileArgs& a, long long tile, bool use_tma, Refill&& refill,
+                                        const Sink& sink = Sink{}) {
+        static_assert(!Sink::kActive || OP == kC2RBwd, "output sinks take backward RFFT samples");
         const C* stage = sm + (size_t)TPC * N;
         const long long tr = tile * TPC + slot;
         const bool valid = tr < a.batch;
@@ -523,9 +543,16 @@ struct TileWorker {
             if (valid) {
                 const C* rw = static_cast<const C*>(a.rw);
                 const CxIn<F, IL> in(ib0, ib1, ibase);
+                [[maybe_unused]] const C* hf = static_cast<const C*>(sink.h);
                 for (int k = 1 + lt; k <= N / 2; k += T) {
-                    const C x1 = in[k];
-                    const C x2 = in[N - k];
+                    C x1 = in[k];
+                    C x2 = in[N - k];
+                    if constexpr (Sink::kActive) {
+                        if (hf) {
+                            x1 = cmul_rn(x1, hf[k]);
+                            x2 = cmul_rn(x2, hf[N - k]);
+                        }
+                    }
                     const C w = rw[k];
                     const F c = w.x, s = w.y;
                     const F si = x1.y + x2.y, dr = x1.x - x2.x;
@@ -535,8 +562,14 @@ struct TileWorker {
                     sm[sidx(N - k)] = zm;
                 }
                 if (lt == 0) {
-                    const C x0 = in[0];
-                    const C xm = in[N];
+                    C x0 = in[0];
+                    C xm = in[N];
+                    if constexpr (Sink::kActive) {
+                        if (hf) {
+                            x0 = cmul_rn(x0, hf[0]);
+                            xm = cmul_rn(xm, hf[N]);
+                        }
+                    }
                     sm[sidx(0)] = cx<C>(mul_rn(x0.x + xm.x, (F)0.5), mul_rn(x0.x - xm.x, (F)0.5));
                 }
             }
@@ -731,7 +764,11 @@ struct TileWorker {
                                     if constexpr (kR2C) {
                                         sm[sidx(pos)] = v[u * G.R + s];
                                     } else if (valid) {
-                                        out.put(pos, kFwd ? v[u * G.R + s] : cswap(v[u * G.R + s]));
+                                        if constexpr (Sink::kActive) {
+                                            sink.add(pos, cswap(v[u * G.R + s]));
+                                        } else {
+                                            out.put(pos, kFwd ? v[u * G.R + s] : cswap(v[u * G.R + s]));
+                                        }
                                     }
                                 }
                             }

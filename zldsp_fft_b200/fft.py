@@ -85,6 +85,14 @@ class Plan:
         C.check(self._lib.zlfft_stft_device(self.handle, op, out_layout, signal, int(hop), window, out0, out1,
                                             int(n_frames), int(out_stride), stream))
 
+    def istft(self, in_layout, in0, in1, hop, n_frames, signal, filter=None, window=None, in_stride=0, stream=0):
+        """Inverse STFT with overlap-add of device bins (zlfft_istft_device):
+        signal[f*hop + n] = sum over frames f, in order, of
+        window[n] * backward(filter * bins_f)[n]; the signal holds
+        (n_frames - 1) * hop + N reals and is written, not accumulated into."""
+        C.check(self._lib.zlfft_istft_device(self.handle, in_layout, in0, in1, int(in_stride), filter, window, int(hop),
+                                             int(n_frames), signal, stream))
+
     def exec_host(self, op, in_layout, out_layout, in0, in1, out0, out1, batch=1):
         C.check(self._lib.zlfft_exec_host_batched(self.handle, op, in_layout, out_layout, in0, in1, out0, out1,
                                                   int(batch)))
