@@ -882,10 +882,11 @@ class Stft:
     desc = ("STFT: 2^27-sample float signal, 4096-point Hann frames at hop 1024 (131,069 frames), "
             "forward_sqr_mag, fused framing + window + RFFT")
     l2 = "each step reads 512 MiB and writes 1.07 GB, > 10x L2 (no L2 flush needed)"
-    order, hop, total = 12, 1024, 1 << 27
+    order, hop = 12, 1024
     dtype = "f32"
 
-    def __init__(self):
+    def __init__(self, total_log2=27):
+        self.total = 1 << total_log2
         n = 1 << self.order
         self.frame_n = n
         self.nf = (self.total - n) // self.hop + 1
@@ -1002,10 +1003,11 @@ class Istft:
     desc = ("inverse STFT: 131,069 frames of 4096-point bins (complex64 AoS), spectral filter, RFFT backward, "
             "Hann synthesis window, overlap-add at hop 1024 into a 2^27-sample signal, fused")
     l2 = "each step reads 2.15 GB and writes 512 MiB, > 20x L2 (no L2 flush needed)"
-    order, hop, total = 12, 1024, 1 << 27
+    order, hop = 12, 1024
     dtype = "f32"
 
-    def __init__(self):
+    def __init__(self, total_log2=27):
+        self.total = 1 << total_log2
         n = 1 << self.order
         self.frame_n = n
         self.nf = (self.total - n) // self.hop + 1
@@ -1334,8 +1336,9 @@ def main():
                     help="cfft2g only: the autotuned form per order (default), the plain form (the reference's "
                          "arithmetic), the fast-twiddle form, or the tensor-core split FP16 hi/lo form")
     ap.add_argument("--total-log2", type=int, default=None,
-                    help="cfft2g only: complex elements per order = 2^k (default 28 = 2 GiB); smaller cases "
-                         "are for profiling and are not the benchmark configuration")
+                    help="cfft2g: complex elements per order = 2^k (default 28 = 2 GiB); stft / istft: signal "
+                         "samples = 2^k (default 27); smaller cases are for profiling and are not the benchmark "
+                         "configuration")
     args = ap.parse_args()
     wl_cls = WORKLOADS[args.workload]
     if args.workload == "cfft2g" and (args.total_log2 is not None or args.form != "tuned"):
@@ -1343,6 +1346,10 @@ def main():
         tl = args.total_log2 if args.total_log2 is not None else 28
         wl_cls = lambda: base(total_log2=tl, form=args.form)  # noqa: E731
         wl_cls.__name__ = base.__name__
+    if args.workload in ("stft", "istft") and args.total_log2 is not None:
+        base_s = wl_cls
+        wl_cls = lambda: base_s(total_log2=args.total_log2)  # noqa: E731
+        wl_cls.__name__ = base_s.__name__
     if args.workload == "mixed" and args.no_autotune:
         base_m = wl_cls
         wl_cls = lambda: base_m(autotune=False)  # noqa: E731

@@ -646,6 +646,8 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     }
 
     const int dop = device_op_code(p, op);
+    // backward RFFT tiles stage their bins by cp.async: element alignment suffices
+    if (dop == zlfft::kC2RBwd) a.tma = p->use_tma ? 1 : 0;
     const int P = p->cfft_order;
     zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
     if (P > zlfft::kTileMaxP) {

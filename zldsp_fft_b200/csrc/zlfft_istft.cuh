@@ -66,7 +66,11 @@ struct IstftCfg {
     static constexpr int N = 1 << P;                  // complex points (frame length / 2)
     static constexpr int T = N / tile_elems(P);       // one transform per CTA
     using Tile = TileCfg<F, P, kC2RBwd, (T > 0 ? T : 1)>;
-    static constexpr size_t SMEM = Tile::XBYTES + (size_t)N * sizeof(C);  // exchange + ring
+    // exchange, then the ring. The bins are read directly: staging them costs
+    // a resident CTA here and measured no faster (the frame rate of the
+    // transform bounds this kernel).
+    static constexpr size_t RING = Tile::XBYTES;
+    static constexpr size_t SMEM = RING + (size_t)N * sizeof(C);
     // whole warps, and the exchange and ring in shared memory
     static constexpr bool kOK = T >= 32 && Tile::TPC == 1 && SMEM <= 200 * 1024;
     static constexpr int MINB = Tile::MINB;
@@ -81,7 +85,7 @@ __global__ void __launch_bounds__(IstftCfg<F, P>::T, IstftCfg<F, P>::MINB)
     constexpr int N = Cfg::N, T = Cfg::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     W wk(a, smem_raw);
-    C* ring = reinterpret_cast<C*>(smem_raw + Cfg::Tile::XBYTES);
+    C* ring = reinterpret_cast<C*>(smem_raw + Cfg::RING);
     C* sig = static_cast<C*>(o.sig);
     const long long hp = o.hop / 2;  // hop in sample pairs
     const long long m0 = (long long)blockIdx.x * o.run;

@@ -158,15 +158,26 @@ struct TileCfg {
     static constexpr int TPC = T >= BLOCK ? 1 : BLOCK / T;
     static constexpr int THREADS = T * TPC;
     static constexpr size_t XBYTES = (size_t)TPC * N * sizeof(C);  // exchange buffer
-    // Staging buffer for the next tile's input, filled by TMA bulk copies
-    // while the current tile computes (not for the RFFT backward, whose
-    // pre-step reads the bins directly).
-    static constexpr bool kTMA = P >= 4 && OP != kC2RBwd && 2 * XBYTES <= 200 * 1024;
-    static constexpr size_t SMEM = XBYTES * (kTMA ? 2 : 1) + (kTMA ? 16 : 0);
-    static constexpr int NG = tile_num_groups(P);
     // Register budget: enough resident CTAs for ~96 registers per thread in
     // FP32 (the last group's 15 complex twiddles stay in registers), ~128 in FP64.
     static constexpr int REGS = sizeof(F) == 4 ? (((OP == kC2CFwd || OP == kC2CBwd) && P >= 10) ? 128 : 96) : 128;
+    // Staging buffer for the next tile's input, filled by TMA bulk copies
+    // while the current tile computes (not for the RFFT backward, whose
+    // pre-step reads the bins).
+    static constexpr bool kTMA = P >= 4 && OP != kC2RBwd && 2 * XBYTES <= 200 * 1024;
+    // Backward RFFT: the next tile's bins (TPC frames of N + 1 complex; SoA:
+    // a re row then an im row per frame) are copied into the staging buffer
+    // by cp.async while the current tile computes (dense bin arrays put odd
+    // frames off the 16-byte alignment bulk copies need). Measured per order
+    // (FP32, GB/s, AoS): complex order 9: 2848 -> 3210, 11: 2879 -> 3300,
+    // 12: 2214 -> 2986, 13: 1848 -> 2346; but 8: 4533 -> 3770 and 10: 3910 ->
+    // 3482, where the extra copy and shared-memory read outweigh the hidden
+    // latency. FP64 keeps direct loads (its buffers would cost resident CTAs).
+    static constexpr size_t BBYTES = ((size_t)TPC * (N + 1) * sizeof(C) + 15) / 16 * 16;
+    static constexpr bool kStageBins = OP == kC2RBwd && sizeof(F) == 4 && (P == 9 || (P >= 11 && P <= 13)) &&
+                                       XBYTES + BBYTES <= 200 * 1024;
+    static constexpr size_t SMEM = kTMA ? 2 * XBYTES + 16 : XBYTES + (kStageBins ? BBYTES : 0);
+    static constexpr int NG = tile_num_groups(P);
     static constexpr int MINB = (65536 / (THREADS * REGS)) > 0 ? (65536 / (THREADS * REGS)) : 1;
 };
 
@@ -509,10 +520,39 @@ struct TileWorker {
 
     __device__ __forceinline__ uint32_t sidx(int pos) const { return swz<C>(sbase + (uint32_t)pos); }
 
+    // Backward RFFT: issue the cp.async copies of tile t's bins into the
+    // staging buffer (all threads share them) and commit them as one group.
+    __device__ __forceinline__ void stage_bins(const TileArgs& a, long long t) const {
+        if constexpr (Cfg::kStageBins) {
+            F* st = reinterpret_cast<F*>(sm + (size_t)TPC * N);
+            for (int q = 0; q < TPC; ++q) {
+                const long long tr = t * TPC + q;
+                if (tr >= a.batch) break;
+                F* d = st + (size_t)q * 2 * (N + 1);
+                const long long base = tr * a.in_stride;
+                if constexpr (IL == kSoA) {
+                    const F* re = static_cast<const F*>(a.in0) + base;
+                    const F* im = static_cast<const F*>(a.in1) + base;
+                    for (int i = (int)threadIdx.x; i <= N; i += Cfg::THREADS) {
+                        cp_async<sizeof(F)>(d + i, re + i);
+                        cp_async<sizeof(F)>(d + N + 1 + i, im + i);
+                    }
+                } else {
+                    const C* src = static_cast<const C*>(a.in0) + base;
+                    C* dc = reinterpret_cast<C*>(d);
+                    for (int i = (int)threadIdx.x; i <= N; i += Cfg::THREADS) cp_async<sizeof(C)>(dc + i, src + i);
+                }
+            }
+            cp_async_commit();
+        }
+    }
+
     // Process tile `tile`. With use_tma, group 0 reads this tile's input from
     // the staging buffer that follows the exchange buffer in shared memory
-    // (placed there by TMA) and calls refill() once done. A backward RFFT may
-    // hand its output samples to `sink` (see NoSink).
+    // (placed there by TMA) and calls refill() once done; for a backward RFFT,
+    // use_tma means the pre-step reads the bins staged by stage_bins (it
+    // waits for them) and calls refill() once they are read. A backward RFFT
+    // may hand its output samples to `sink` (see NoSink).
     template <class Refill, class Sink = NoSink>
     __device__ __forceinline__ void run(const TileArgs& a, long long tile, bool use_tma, Refill&& refill,
                                         const Sink& sink = Sink{}) {
@@ -540,13 +580,32 @@ struct TileWorker {
         // ------------------------------------------------ input
         if constexpr (OP == kC2RBwd) {
             // Backward RFFT pre-step into shared memory (execute.hpp:399-451).
+            if constexpr (Cfg::kStageBins) {
+                if (use_tma) {  // this tile's bins are in the staging buffer
+                    cp_async_wait_all();
+                    __syncthreads();
+                }
+            }
             if (valid) {
                 const C* rw = static_cast<const C*>(a.rw);
                 const CxIn<F, IL> in(ib0, ib1, ibase);
                 [[maybe_unused]] const C* hf = static_cast<const C*>(sink.h);
+                [[maybe_unused]] const F* sb = reinterpret_cast<const F*>(stage) + (size_t)slot * 2 * (N + 1);
+                auto bin = [&](int k) -> C {
+                    if constexpr (Cfg::kStageBins) {
+                        if (use_tma) {
+                            if constexpr (IL == kSoA) {
+                                return cx<C>(sb[k], sb[N + 1 + k]);
+                            } else {
+                                return reinterpret_cast<const C*>(sb)[k];
+                            }
+                        }
+                    }
+                    return in[k];
+                };
                 for (int k = 1 + lt; k <= N / 2; k += T) {
-                    C x1 = in[k];
-                    C x2 = in[N - k];
+                    C x1 = bin(k);
+                    C x2 = bin(N - k);
                     if constexpr (Sink::kActive) {
                         if (hf) {
                             x1 = cmul_rn(x1, hf[k]);
@@ -562,8 +621,8 @@ struct TileWorker {
                     sm[sidx(N - k)] = zm;
                 }
                 if (lt == 0) {
-                    C x0 = in[0];
-                    C xm = in[N];
+                    C x0 = bin(0);
+                    C xm = bin(N);
                     if constexpr (Sink::kActive) {
                         if (hf) {
                             x0 = cmul_rn(x0, hf[0]);
@@ -574,6 +633,9 @@ struct TileWorker {
                 }
             }
             __syncthreads();
+            if constexpr (Cfg::kStageBins) {
+                if (use_tma) refill();  // the staged bins are read: the next tile's may come in
+            }
         }
 
         // ------------------------------------------------ stage groups
@@ -859,6 +921,9 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
         }
     }
     uint32_t phase = 0;
+    // backward RFFT: bins staged by cp.async, one tile ahead
+    const bool use_stage = Cfg::kStageBins && !GATHER && a.tma;
+    if (use_stage) w.stage_bins(a, blockIdx.x);
 
     for (long long tile = blockIdx.x; tile * TPC < a.batch; tile += gridDim.x) {
         if constexpr (Cfg::kTMA) {
@@ -872,11 +937,15 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
                 phase ^= 1u;
             }
         }
-        w.run(a, tile, use_tma, [&]() {
-            fence_proxy_async_smem();  // reads of the staging buffer before its TMA refill
-            __syncthreads();           // staging fully read: refill it with the next tile
-            issue(tile + gridDim.x);
-        });
+        if constexpr (OP == kC2RBwd) {
+            w.run(a, tile, use_stage, [&]() { w.stage_bins(a, tile + gridDim.x); });
+        } else {
+            w.run(a, tile, use_tma, [&]() {
+                fence_proxy_async_smem();  // reads of the staging buffer before its TMA refill
+                __syncthreads();           // staging fully read: refill it with the next tile
+                issue(tile + gridDim.x);
+            });
+        }
     }
 }
 
