@@ -73,8 +73,9 @@ typedef struct zlfft_plan_s* zlfft_plan;
  * Replaces the constructors CFFT<F>::CFFT(size_t order)
  * (src/zldsp_fft_cfft.hpp:19-23) and RFFT<F>::RFFT(size_t order)
  * (src/zldsp_fft_rfft.hpp:24-53). order is log2 of the transform length N
- * (RFFT: real length). Twiddle tables are generated on the device in FP64 and
- * rounded to the plan's precision. device < 0 means the current device. */
+ * (RFFT: real length): CFFT orders 0-26, RFFT orders 1-27 (ZLFFT_ERR_UNSUPPORTED
+ * above). Twiddle tables are generated on the device in FP64 and rounded to
+ * the plan's precision. device < 0 means the current device. */
 ZLFFT_API int zlfft_plan_create(zlfft_plan* plan, int kind, int precision, size_t order, int mode, int device);
 
 /* Release a plan and every buffer it owns. Replaces the reference objects'

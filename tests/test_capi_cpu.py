@@ -72,7 +72,7 @@ def test_mixed_batch_descriptors_rejected_without_cuda():
     assert lib.zlfft_mixed_create(ctypes.byref(h), None, 3, -1) == C.ERR_INVALID_ARG
     assert one(kind=5) == C.ERR_INVALID_ARG and "descriptor 1" in C.last_error()
     assert one(precision=9) == C.ERR_INVALID_ARG
-    assert one(order=25) == C.ERR_UNSUPPORTED
+    assert one(order=27) == C.ERR_UNSUPPORTED  # above the three-pass maximum (26)
     assert one(kind=C.R2C, order=0) == C.ERR_UNSUPPORTED  # RFFT order 0 has no inner CFFT
     assert one(op=7) == C.ERR_INVALID_ARG
     assert one(op=C.FORWARD_SQR_MAG) == C.ERR_INVALID_ARG  # an RFFT operation

@@ -150,6 +150,7 @@ struct TablesHolder {
         zlfft::fill_istft_f64(i64);
         zlfft::fill_tc_pass_a(tc);
         zlfft::fill_tc_pass_b(tc);
+        zlfft::fill_tc_pass_c(tc);
         zlfft::fill_gather_f32(g32);
         zlfft::fill_gather_f64(g64);
         zlfft::fill_tile_c2c_f32(f32);
@@ -158,8 +159,10 @@ struct TablesHolder {
         zlfft::fill_tile_r2c_f64(f64);
         zlfft::fill_pass_f32_a(p32);
         zlfft::fill_pass_f32_b(p32);
+        zlfft::fill_pass_f32_c(p32);
         zlfft::fill_pass_f64_a(p64);
         zlfft::fill_pass_f64_b(p64);
+        zlfft::fill_pass_f64_c(p64);
     }
 };
 

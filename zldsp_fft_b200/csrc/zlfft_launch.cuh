@@ -100,7 +100,7 @@ void fill_gather_f64(GatherTable& t);
 
 // ------------------------------------------------------------------ multi-pass
 constexpr int kPassMinP = 14;
-constexpr int kPassMaxP = 24;
+constexpr int kPassMaxP = 26;  // three passes reach order 26
 constexpr int kMaxPasses = 3;
 
 using PassLaunchFn = cudaError_t (*)(const PassArgs&, cudaStream_t, const LaunchCtx&);
@@ -285,8 +285,10 @@ void fill_pass_orders(PassTable& t, std::integer_sequence<int, Ps...>) {
 // ranges split over translation units for parallel builds
 void fill_pass_f32_a(PassTable& t);  // orders 14..18
 void fill_pass_f32_b(PassTable& t);  // orders 19..24
+void fill_pass_f32_c(PassTable& t);  // orders 25..26
 void fill_pass_f64_a(PassTable& t);
 void fill_pass_f64_b(PassTable& t);
+void fill_pass_f64_c(PassTable& t);
 
 template <typename F, int Lo, int Hi, int... Ps>
 void fill_pass_range_impl(PassTable& t, std::integer_sequence<int, Ps...>) {
@@ -373,6 +375,7 @@ void fill_tc_pass_range_impl(TcPassTable& t, std::integer_sequence<int, Ps...>) 
 }
 void fill_tc_pass_a(TcPassTable& t);  // orders 14..18
 void fill_tc_pass_b(TcPassTable& t);  // orders 19..24
+void fill_tc_pass_c(TcPassTable& t);  // orders 25..26
 
 // Each translation unit fills its part of a precision's table.
 void fill_tile_c2c_f32(TileTable& t);

@@ -2,5 +2,5 @@
 #include "zlfft_launch.cuh"
 
 namespace zlfft {
-void fill_pass_f64_b(PassTable& t) { fill_pass_range<double, 19, kPassMaxP>(t); }
+void fill_pass_f64_b(PassTable& t) { fill_pass_range<double, 19, 24>(t); }
 }  // namespace zlfft
