@@ -578,63 +578,80 @@ struct TileWorker {
         C v[E];
 
         // ------------------------------------------------ input
+        // Backward RFFT pre-step (execute.hpp:399-451): Z[p] from the bins at p
+        // and N - p. Where the bins are staged in shared memory (and no sink is
+        // attached), each thread computes the Z of its own group-0 positions in
+        // registers (bin pair k, N - k is read by the two threads that need it),
+        // so Z never goes through shared memory. Elsewhere Z is built in shared
+        // memory first: reading each bin twice from global memory measured
+        // 20-50% slower (FP32 orders 7-9 and 11, FP64, the inverse STFT), while
+        // the staged orders gained 3-9% (RFFT<float> backward order 13: 3018 ->
+        // 3301 GB/s, order 14: 2342 -> 2558).
+        constexpr bool kDirectPre = OP == kC2RBwd && NG >= 2 && Cfg::kStageBins && !Sink::kActive;
+        [[maybe_unused]] const C* rw = static_cast<const C*>(a.rw);
+        [[maybe_unused]] const C* hf = static_cast<const C*>(sink.h);
+        [[maybe_unused]] const F* sb = reinterpret_cast<const F*>(stage) + (size_t)slot * 2 * (N + 1);
+        [[maybe_unused]] const CxIn<F, IL> bins(ib0, ib1, ibase);
+        [[maybe_unused]] auto bin = [&](int k) -> C {  // bin k, times the filter's bin k
+            C x;
+            if constexpr (Cfg::kStageBins) {
+                if (use_tma) {
+                    if constexpr (IL == kSoA) {
+                        x = cx<C>(sb[k], sb[N + 1 + k]);
+                    } else {
+                        x = reinterpret_cast<const C*>(sb)[k];
+                    }
+                } else {
+                    x = bins[k];
+                }
+            } else {
+                x = bins[k];
+            }
+            if constexpr (Sink::kActive) {
+                if (hf) x = cmul_rn(x, hf[k]);
+            }
+            return x;
+        };
+        // Z[p]: p = 0 from bins 0 and N; 1 <= p < N/2 the first value of pair
+        // k = p, N/2 <= p < N the second value of pair k = N - p
+        [[maybe_unused]] auto prez = [&](int p) -> C {
+            if (p == 0) {
+                const C x0 = bin(0), xm = bin(N);
+                return cx<C>(mul_rn(x0.x + xm.x, (F)0.5), mul_rn(x0.x - xm.x, (F)0.5));
+            }
+            const int k = p < N / 2 ? p : N - p;
+            const C x1 = bin(k), x2 = bin(N - k);
+            const C w = rw[k];
+            const F c = w.x, s = w.y;
+            const F si = x1.y + x2.y, dr = x1.x - x2.x;
+            if (p < N / 2) return cx<C>(fma_rn(-dr, s, fma_rn(-si, c, x1.x)), fma_rn(dr, c, fma_rn(-si, s, x1.y)));
+            return cx<C>(fma_rn(dr, s, fma_rn(si, c, x2.x)), fma_rn(dr, c, fma_rn(-si, s, x2.y)));
+        };
         if constexpr (OP == kC2RBwd) {
-            // Backward RFFT pre-step into shared memory (execute.hpp:399-451).
             if constexpr (Cfg::kStageBins) {
                 if (use_tma) {  // this tile's bins are in the staging buffer
                     cp_async_wait_all();
                     __syncthreads();
                 }
             }
-            if (valid) {
-                const C* rw = static_cast<const C*>(a.rw);
-                const CxIn<F, IL> in(ib0, ib1, ibase);
-                [[maybe_unused]] const C* hf = static_cast<const C*>(sink.h);
-                [[maybe_unused]] const F* sb = reinterpret_cast<const F*>(stage) + (size_t)slot * 2 * (N + 1);
-                auto bin = [&](int k) -> C {
-                    if constexpr (Cfg::kStageBins) {
-                        if (use_tma) {
-                            if constexpr (IL == kSoA) {
-                                return cx<C>(sb[k], sb[N + 1 + k]);
-                            } else {
-                                return reinterpret_cast<const C*>(sb)[k];
-                            }
-                        }
+            if constexpr (!kDirectPre) {
+                if (valid) {  // one thread per bin pair (k, N - k): both Z values from one read of the pair
+                    for (int k = 1 + lt; k <= N / 2; k += T) {
+                        const C x1 = bin(k), x2 = bin(N - k);
+                        const C w = rw[k];
+                        const F c = w.x, s = w.y;
+                        const F si = x1.y + x2.y, dr = x1.x - x2.x;
+                        const C zk = cx<C>(fma_rn(-dr, s, fma_rn(-si, c, x1.x)), fma_rn(dr, c, fma_rn(-si, s, x1.y)));
+                        const C zm = cx<C>(fma_rn(dr, s, fma_rn(si, c, x2.x)), fma_rn(dr, c, fma_rn(-si, s, x2.y)));
+                        if (k != N / 2) sm[sidx(k)] = zk;
+                        sm[sidx(N - k)] = zm;
                     }
-                    return in[k];
-                };
-                for (int k = 1 + lt; k <= N / 2; k += T) {
-                    C x1 = bin(k);
-                    C x2 = bin(N - k);
-                    if constexpr (Sink::kActive) {
-                        if (hf) {
-                            x1 = cmul_rn(x1, hf[k]);
-                            x2 = cmul_rn(x2, hf[N - k]);
-                        }
-                    }
-                    const C w = rw[k];
-                    const F c = w.x, s = w.y;
-                    const F si = x1.y + x2.y, dr = x1.x - x2.x;
-                    const C zk = cx<C>(fma_rn(-dr, s, fma_rn(-si, c, x1.x)), fma_rn(dr, c, fma_rn(-si, s, x1.y)));
-                    const C zm = cx<C>(fma_rn(dr, s, fma_rn(si, c, x2.x)), fma_rn(dr, c, fma_rn(-si, s, x2.y)));
-                    if (k != N / 2) sm[sidx(k)] = zk;
-                    sm[sidx(N - k)] = zm;
+                    if (lt == 0) sm[sidx(0)] = prez(0);
                 }
-                if (lt == 0) {
-                    C x0 = bin(0);
-                    C xm = bin(N);
-                    if constexpr (Sink::kActive) {
-                        if (hf) {
-                            x0 = cmul_rn(x0, hf[0]);
-                            xm = cmul_rn(xm, hf[N]);
-                        }
-                    }
-                    sm[sidx(0)] = cx<C>(mul_rn(x0.x + xm.x, (F)0.5), mul_rn(x0.x - xm.x, (F)0.5));
+                __syncthreads();
+                if constexpr (Cfg::kStageBins) {
+                    if (use_tma) refill();  // the staged bins are read: the next tile's may come in
                 }
-            }
-            __syncthreads();
-            if constexpr (Cfg::kStageBins) {
-                if (use_tma) refill();  // the staged bins are read: the next tile's may come in
             }
         }
 
@@ -671,7 +688,15 @@ struct TileWorker {
                         constexpr int NB = E / G.R;
                         constexpr bool kLast = (GI + 1 == NG);
                         // ---- inputs of this group
-                        if constexpr (GI == 0 && OP != kC2RBwd) {
+                        if constexpr (GI == 0 && kDirectPre) {
+#pragma unroll
+                            for (int u = 0; u < NB; ++u) {
+                                const int b = lt + u * T;
+#pragma unroll
+                                for (int rho = 0; rho < G.R; ++rho)
+                                    v[u * G.R + rho] = valid ? cswap(prez(b + rho * (N / G.R))) : cx<C>((F)0, (F)0);
+                            }
+                        } else if constexpr (GI == 0 && OP != kC2RBwd) {
                             if (use_tma) {
                                 const C* sc = stage + (size_t)slot * N;
                                 const F* sf = reinterpret_cast<const F*>(sc);
@@ -751,6 +776,9 @@ struct TileWorker {
                         // ---- outputs
                         if constexpr (!kLast) {
                             __syncthreads();
+                            if constexpr (GI == 0 && kDirectPre && Cfg::kStageBins) {
+                                if (use_tma) refill();  // the staged bins are read: the next tile's may come in
+                            }
 #pragma unroll
                             for (int u = 0; u < NB; ++u) {
                                 const int b = lt + u * T;
