@@ -400,14 +400,25 @@ int ensure_scratch(zlfft_plan_s* p) {
     return ZLFFT_OK;
 }
 
+// Grid of the RFFT split / pre-step kernels: x covers one transform's M/2 + 1
+// bin pairs in blocks of 256; y strides over the batch, with about 16 blocks
+// per SM in all.
+dim3 pair_grid(const zlfft_plan_s* p, int M, long long batch) {
+    const long long gx = (M / 2 + 1 + 255) / 256;
+    long long gy = ((long long)p->num_sms * 16 + gx - 1) / gx;
+    if (gy > batch) gy = batch;
+    if (gy > 65535) gy = 65535;
+    if (gy < 1) gy = 1;
+    return dim3((unsigned)gx, (unsigned)gy, 1);
+}
+
 template <typename F>
 cudaError_t launch_split(const zlfft_plan_s* p, int dop, int out_layout, const void* z, void* o0, void* o1,
                          long long batch, long long out_stride, cudaStream_t st, const zlfft::LaunchCtx& ctx,
                          void* const* go0 = nullptr, void* const* go1 = nullptr) {
     using C = zlfft::Cx<F>;
     const int M = 1 << p->cfft_order;
-    const long long total = (long long)(M / 2 + 1) * batch;
-    const unsigned grid = (unsigned)std::min<long long>((total + 255) / 256, (long long)p->num_sms * 16);
+    const dim3 grid = pair_grid(p, M, batch);
     const C* zc = static_cast<const C*>(z);
     const C* rw = static_cast<const C*>(p->d_rw);
     if (dop == zlfft::kR2CSqrMag)
@@ -426,8 +437,7 @@ cudaError_t launch_pre(const zlfft_plan_s* p, int in_layout, const void* i0, con
                        const void* const* gi0 = nullptr, const void* const* gi1 = nullptr) {
     using C = zlfft::Cx<F>;
     const int M = 1 << p->cfft_order;
-    const long long total = (long long)(M / 2 + 1) * batch;
-    const unsigned grid = (unsigned)std::min<long long>((total + 255) / 256, (long long)p->num_sms * 16);
+    const dim3 grid = pair_grid(p, M, batch);
     const C* rw = static_cast<const C*>(p->d_rw);
     if (in_layout == ZLFFT_AOS)
         zlfft::rfft_pre_kernel<F, zlfft::kAoS><<<grid, 256, 0, st>>>(i0, i1, static_cast<C*>(z), rw, M, batch, in_stride, M, gi0, gi1);

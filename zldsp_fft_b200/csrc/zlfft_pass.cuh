@@ -497,16 +497,17 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
 // N/2-point spectrum Z (AoS, natural order) and writes bins (or squared
 // magnitudes); the backward pre-step writes Z from bins
 // (src/common/zldsp_fft_common_execute.hpp:318-368, :481-536, :399-451).
-// One thread per bin pair (k, M - k), k = 0 .. M/2 (k = 0 is DC/Nyquist).
+// One thread per bin pair (k, M - k), k = 0 .. M/2 (k = 0 is DC/Nyquist):
+// grid x covers the pairs of a transform, grid y strides over the transforms
+// (no 64-bit division per element).
 template <typename F, int OP, int LAYOUT>
 __global__ void rfft_split_kernel(const Cx<F>* z, void* out0, void* out1, const Cx<F>* rw, int M, long long batch,
                                   long long z_stride, long long out_stride, void* const* gout0, void* const* gout1) {
     using C = Cx<F>;
-    const long long pairs = (long long)(M / 2 + 1);
-    const long long total = pairs * batch;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        const long long tr = i / pairs;
-        const int k = (int)(i % pairs);
+    const int k = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (k > M / 2) return;
+    const C w = k > 0 ? rw[k] : cx<C>((F)0, (F)0);  // the pair's twiddles, for every transform
+    for (long long tr = blockIdx.y; tr < batch; tr += gridDim.y) {
         const C* zt = z + tr * z_stride;
         constexpr int OL2 = (OP == kR2CSqrMag) ? (int)kAoS : LAYOUT;
         void* o0 = gout0 ? gout0[tr] : out0;
@@ -526,7 +527,6 @@ __global__ void rfft_split_kernel(const Cx<F>* z, void* out0, void* out1, const 
             }
             continue;
         }
-        const C w = rw[k];
         const SplitOut<F> o = rfft_split<F>(zt[k], zt[M - k], w.x, w.y);
         if constexpr (OP == kR2CFwd) {
             if (k != M / 2) out.put(k, cx<C>(o.xr_k, o.xi_k));
@@ -543,11 +543,10 @@ __global__ void rfft_pre_kernel(const void* in0, const void* in1, Cx<F>* z, cons
                                 long long in_stride, long long z_stride, const void* const* gin0,
                                 const void* const* gin1) {
     using C = Cx<F>;
-    const long long pairs = (long long)(M / 2 + 1);
-    const long long total = pairs * batch;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        const long long tr = i / pairs;
-        const int k = (int)(i % pairs);
+    const int k = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (k > M / 2) return;
+    const C w = k > 0 ? rw[k] : cx<C>((F)0, (F)0);  // the pair's twiddles, for every transform
+    for (long long tr = blockIdx.y; tr < batch; tr += gridDim.y) {
         const CxIn<F, LAYOUT> in(gin0 ? gin0[tr] : in0, gin0 ? (gin1 ? gin1[tr] : nullptr) : in1,
                                  gin0 ? 0 : tr * in_stride);
         C* zt = z + tr * z_stride;
@@ -557,7 +556,6 @@ __global__ void rfft_pre_kernel(const void* in0, const void* in1, Cx<F>* z, cons
             continue;
         }
         const C x1 = in[k], x2 = in[M - k];
-        const C w = rw[k];
         const F c = w.x, s = w.y;
         const F si = x1.y + x2.y, dr = x1.x - x2.x;
         const C zk = cx<C>(fma_rn(-dr, s, fma_rn(-si, c, x1.x)), fma_rn(dr, c, fma_rn(-si, s, x1.y)));
