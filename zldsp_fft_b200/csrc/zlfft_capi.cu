@@ -295,6 +295,7 @@ struct zlfft_plan_s {
     bool tc_form = false;   // 256-point passes in the tensor-core split form
     bool fast_form = false; // multi-pass radix-16 groups with fast twiddles (ZLFFT_MODE_FAST)
     bool fuse_split = false;  // RFFT forward: split fused into the last pass (else its own kernel)
+    bool tile14 = true;       // RFFT<float> real order 15 as one tile per transform (rfft_tile14)
     int store_tma = -1;       // first pass output by TMA tensor stores (-1: the precision's default)
     std::mutex mu;
 };
@@ -604,6 +605,14 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
     return ZLFFT_OK;
 }
 
+// RFFT<float> of real order 15 (complex order 14) runs as one tile per
+// transform: one pass over HBM with the split fused, against two passes and a
+// split kernel (+18-26% measured, forward, backward and squared magnitudes).
+// The tensor-core form keeps its multi-pass passes.
+bool rfft_tile14(const zlfft_plan_s* p) {
+    return p->cfft_order == 14 && p->kind == ZLFFT_R2C && p->prec == ZLFFT_F32 && !p->tc_form && p->tile14;
+}
+
 int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,
                      void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, cudaStream_t stream) {
     int rc = validate_op(p, op, in_layout, out_layout);
@@ -663,7 +672,7 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     if (dop == zlfft::kC2RBwd) a.tma = p->use_tma ? 1 : 0;
     const int P = p->cfft_order;
     zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
-    if (P > zlfft::kTileMaxP) {
+    if (P > zlfft::kTileMaxP && !rfft_tile14(p)) {
         DeviceGuard g(p->device);
         return exec_multipass(p, dop, in_layout, out_layout, a, stream, ctx);
     }
@@ -1177,7 +1186,8 @@ bool mixed_in_persistent(const MixedGroupHost& g) { return g.P >= zlfft::kMixedM
 int mixed_run_group(zlfft_mixed_s* m, const MixedGroupHost& g, cudaStream_t st) {
     zlfft::LaunchCtx ctx{m->num_sms, &m->launches};
     const zlfft::TileArgs a = mixed_args(m, g);
-    if (g.P > zlfft::kTileMaxP) return exec_multipass(g.plan, g.dop, ZLFFT_AOS, ZLFFT_AOS, a, st, ctx);
+    if (g.P > zlfft::kTileMaxP && !rfft_tile14(g.plan))
+        return exec_multipass(g.plan, g.dop, ZLFFT_AOS, ZLFFT_AOS, a, st, ctx);
     const zlfft::GatherTable& t = g.prec == ZLFFT_F32 ? tables().g32 : tables().g64;
     zlfft::TileLaunchFn fn = t.fn[g.P][g.dop];
     if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no gathered kernel for order %d", g.P);

@@ -4,6 +4,6 @@
 
 namespace zlfft {
 void fill_gather_f32(GatherTable& t) {
-    fill_gather_orders<float>(t, std::make_integer_sequence<int, kTileMaxP + 1>{});
+    fill_gather_orders<float>(t, std::make_integer_sequence<int, kTileMaxP_f32 + 1>{});
 }
 }  // namespace zlfft

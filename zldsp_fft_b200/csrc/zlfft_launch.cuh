@@ -16,9 +16,14 @@
 
 namespace zlfft {
 
-constexpr int kTileMaxP_f32 = 13;  // tile kernel: whole transform in one CTA
+constexpr int kTileMaxP_f32 = 14;  // tile kernel: whole transform in one CTA
 constexpr int kTileMaxP_f64 = 13;
-constexpr int kTileMaxP = 13;
+constexpr int kTileMaxP = 13;      // orders every path treats as single-CTA
+// FP32 order 14 (128 KB, one CTA per SM) has tile kernels too: the RFFT of
+// real order 15 runs on them from the batched and mixed entry points (one
+// pass over HBM instead of two passes and a split kernel); the CFFT of order
+// 14 measured faster as two passes and stays multi-pass.
+constexpr int kTileTableP = 14;
 
 struct LaunchCtx {
     int num_sms;
@@ -29,13 +34,13 @@ using TileLaunchFn = cudaError_t (*)(const TileArgs&, cudaStream_t, const Launch
 
 struct TileTable {
     // [order][op][in_layout][out_layout]
-    TileLaunchFn fn[kTileMaxP + 1][5][2][2];
+    TileLaunchFn fn[kTileTableP + 1][5][2][2];
     // STFT front end: RFFT forward with the window multiplied in at load,
     // [order][0: forward, 1: forward_sqr_mag][out_layout]
-    TileLaunchFn stft[kTileMaxP + 1][2][2];
+    TileLaunchFn stft[kTileTableP + 1][2][2];
     // fast-twiddle form of the orders with middle radix-16 groups (11..13),
     // AoS input: [order][op][out_layout]
-    TileLaunchFn fast[kTileMaxP + 1][5][2];
+    TileLaunchFn fast[kTileTableP + 1][5][2];
 };
 
 template <typename F, int P, int OP, int IL, int OL, bool WIN = false, bool FAST = false>
@@ -65,7 +70,7 @@ cudaError_t launch_tile(const TileArgs& a, cudaStream_t stream, const LaunchCtx&
 // Tile kernels reading/writing per-transform pointers (mixed batches), for
 // the AoS <-> AoS operations: [order][op].
 struct GatherTable {
-    TileLaunchFn fn[kTileMaxP + 1][5];
+    TileLaunchFn fn[kTileTableP + 1][5];
 };
 
 template <typename F, int P, int OP>

@@ -153,7 +153,9 @@ template <typename F, int P, int OP = kC2CFwd, int BLOCK = 128>
 struct TileCfg {
     using C = Cx<F>;
     static constexpr int N = 1 << P;
-    static constexpr int E = tile_elems(P);
+    // points per thread: the largest group radix; order 14 takes two radix-16
+    // butterflies per thread per group (512 threads for 16384 points)
+    static constexpr int E = P == 14 ? 2 * tile_elems(P) : tile_elems(P);
     static constexpr int T = N / E;  // threads per transform
     static constexpr int TPC = T >= BLOCK ? 1 : BLOCK / T;
     static constexpr int THREADS = T * TPC;
