@@ -131,7 +131,7 @@ ZLFFT_API int zlfft_exec_device(zlfft_plan plan, int op, int in_layout, int out_
  * out + f*out_stride (0 = dense). One launch: frames are read straight from the
  * signal and windowed as they are loaded; no framed copy is made. window NULL
  * means a rectangular window. hop must be even; the signal must hold
- * (n_frames - 1) * hop + N samples. Frame orders up to 14 (N <= 16384). No
+ * (n_frames - 1) * hop + N samples. Frame orders up to 15 in FP32 (N <= 32768), 14 in FP64. No
  * reference counterpart: a spectrum analyser built on the reference calls
  * forward_sqr_mag frame by frame on copies it windows itself. */
 ZLFFT_API int zlfft_stft_device(zlfft_plan plan, int op, int out_layout, const void* signal, size_t hop,

@@ -40,7 +40,8 @@ def _run(plan, sig, hop, win, nf, op, ol, out_stride=0):
     return (a[..., 0] + 1j * a[..., 1])[:, :nb]
 
 
-@pytest.mark.parametrize("order,hop,nf", [(12, 1024, 40), (12, 6, 25), (8, 2, 300), (14, 4096, 9), (1, 2, 5)])
+@pytest.mark.parametrize("order,hop,nf", [(12, 1024, 40), (12, 6, 25), (8, 2, 300), (14, 4096, 9), (15, 8192, 6),
+                                          (1, 2, 5)])
 def test_stft_f32_bit_exact(oracle, order, hop, nf):
     n = 1 << order
     rng = np.random.default_rng(900 + order)
@@ -86,8 +87,9 @@ def test_stft_rejects_bad_arguments():
                                  None) == Z._capi.ERR_INVALID_ARG  # SoA needs two outputs
     assert lib.zlfft_stft_device(Z.Plan(Z.C2C, 10).handle, Z.FORWARD, Z.AOS, sig.data_ptr(), 4, None,
                                  out.data_ptr(), None, 4, 0, None) == Z._capi.ERR_INVALID_ARG
-    assert lib.zlfft_stft_device(Z.Plan(Z.R2C, 15).handle, Z.FORWARD, Z.AOS, sig.data_ptr(), 4, None,
-                                 out.data_ptr(), None, 1, 0, None) == Z._capi.ERR_UNSUPPORTED
+    for order, dt in ((16, np.float32), (15, np.float64)):  # above the single-CTA frame orders
+        assert lib.zlfft_stft_device(Z.Plan(Z.R2C, order, dt).handle, Z.FORWARD, Z.AOS, sig.data_ptr(), 4, None,
+                                     out.data_ptr(), None, 1, 0, None) == Z._capi.ERR_UNSUPPORTED
     assert lib.zlfft_stft_device(h, Z.FORWARD, Z.AOS, sig.data_ptr() + 4, 4, None, out.data_ptr(), None, 4, 0,
                                  None) == Z._capi.ERR_ALIGNMENT
     assert lib.zlfft_stft_device(h, Z.FORWARD, Z.AOS, sig.data_ptr(), 4, None, out.data_ptr(), None, 0, 0,

@@ -698,8 +698,8 @@ int stft_impl(zlfft_plan_s* p, int op, int out_layout, const void* signal, size_
     if (op != ZLFFT_FORWARD && op != ZLFFT_FORWARD_SQR_MAG)
         return fail(ZLFFT_ERR_INVALID_ARG, "STFT op must be FORWARD or FORWARD_SQR_MAG");
     if (out_layout != ZLFFT_AOS && out_layout != ZLFFT_SOA) return fail(ZLFFT_ERR_INVALID_ARG, "invalid layout");
-    if (p->cfft_order > zlfft::kTileMaxP)
-        return fail(ZLFFT_ERR_UNSUPPORTED, "STFT frames up to order %d", zlfft::kTileMaxP + 1);
+    const int max_pc = p->prec == ZLFFT_F32 ? zlfft::kTileMaxP_f32 : zlfft::kTileMaxP_f64;
+    if (p->cfft_order > max_pc) return fail(ZLFFT_ERR_UNSUPPORTED, "STFT frames up to order %d", max_pc + 1);
     if (hop == 0 || hop % 2) return fail(ZLFFT_ERR_INVALID_ARG, "hop must be even and positive (frames are read as pairs)");
     const bool soa = op == ZLFFT_FORWARD && out_layout == ZLFFT_SOA;
     if (!signal || !out0 || (soa && !out1)) return fail(ZLFFT_ERR_INVALID_ARG, "null buffer pointer");
@@ -1207,16 +1207,23 @@ int mixed_run(zlfft_mixed_s* m, int schedule, cudaStream_t st) {
     }
     // The groups outside the persistent kernel (largest first) are dealt to the
     // side streams, so groups of different orders overlap each other's tails
-    // and the persistent launch on the caller's stream.
+    // and the persistent launch on the caller's stream. The groups of one plan
+    // (one size, several operations; adjacent in the sorted order) share its
+    // scratch, so they are dealt to the same stream, one after another.
     int big = 0;
     for (const MixedGroupHost& g : m->groups) big += mixed_in_persistent(g) ? 0 : 1;
     if (big) {
         ZL_CUDA(cudaEventRecord(m->ev_fork, st));
         for (int i = 0; i < zlfft_mixed_s::kSideStreams; ++i) ZL_CUDA(cudaStreamWaitEvent(m->side[i], m->ev_fork, 0));
-        int k = 0;
+        int si = -1;
+        const zlfft_plan_s* prev = nullptr;
         for (const MixedGroupHost& g : m->groups) {
             if (mixed_in_persistent(g)) continue;
-            int rc = mixed_run_group(m, g, m->side[k++ % zlfft_mixed_s::kSideStreams]);
+            if (g.plan != prev) {
+                si = (si + 1) % zlfft_mixed_s::kSideStreams;
+                prev = g.plan;
+            }
+            int rc = mixed_run_group(m, g, m->side[si]);
             if (rc) return rc;
         }
     }
