@@ -295,7 +295,6 @@ struct zlfft_plan_s {
     bool tc_form = false;   // 256-point passes in the tensor-core split form
     bool fast_form = false; // multi-pass radix-16 groups with fast twiddles (ZLFFT_MODE_FAST)
     bool fuse_split = false;  // RFFT forward: split fused into the last pass (else its own kernel)
-    bool tile14 = true;       // RFFT<float> real order 15 as one tile per transform (rfft_tile14)
     int store_tma = -1;       // first pass output by TMA tensor stores (-1: the precision's default)
     std::mutex mu;
 };
@@ -610,7 +609,7 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
 // split kernel (+18-26% measured, forward, backward and squared magnitudes).
 // The tensor-core form keeps its multi-pass passes.
 bool rfft_tile14(const zlfft_plan_s* p) {
-    return p->cfft_order == 14 && p->kind == ZLFFT_R2C && p->prec == ZLFFT_F32 && !p->tc_form && p->tile14;
+    return p->cfft_order == 14 && p->kind == ZLFFT_R2C && p->prec == ZLFFT_F32 && !p->tc_form;
 }
 
 int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,

@@ -73,6 +73,7 @@ struct IstftCfg {
     static constexpr size_t SMEM = RING + (size_t)N * sizeof(C);
     // whole warps, and the exchange and ring in shared memory
     static constexpr bool kOK = T >= 32 && Tile::TPC == 1 && SMEM <= 200 * 1024;
+    static_assert(!kOK || Tile::THREADS == T, "one transform per CTA of T threads");
     static constexpr int MINB = Tile::MINB;
 };
 
