@@ -1172,20 +1172,46 @@ class Istft:
         return (f"{frames} of {self.nf} frames: numpy filter multiply, the reference's RFFT backward, numpy window "
                 f"and sequential overlap-add, median of 3")
 
+    e2e_slices = 8
+    e2e_api = ("zlfft_istft_device on 8 slices of the frames (each also given the K - 1 frames before it, "
+               "its signal into its own buffer, its final blocks copied back), pinned host buffers, "
+               "H2D / run / D2H pipelined on three streams")
+
     def setup_e2e(self):
         import torch
         self.h_bins = self.bins.cpu().pin_memory()
         self.h_sig = torch.empty(self.total, dtype=torch.float32).pin_memory()
         self.e2e_h2d = self.h_bins.numel() * 4
         self.e2e_d2h = self.h_sig.numel() * 4
+        n, hop, k = self.frame_n, self.hop, self.frame_n // self.hop
+        self.cuts = [self.nf * j // self.e2e_slices for j in range(self.e2e_slices + 1)]
+        # slice [f0, f1) runs frames [g0, f1), g0 = f0 - (K - 1): its blocks [f0, f1) then
+        # hold their final sums (the same terms, in the same order, as one launch)
+        self.slice_sig = [torch.empty((f1 - max(0, f0 - k + 1) - 1) * hop + n, dtype=torch.float32,
+                                      device=self.bins.device) for f0, f1 in zip(self.cuts[:-1], self.cuts[1:])]
+        self.pipe = SlicePipe(self.bins.device)
 
     def e2e_step(self):
-        import torch
-        st = torch.cuda.current_stream()
-        self.bins.copy_(self.h_bins, non_blocking=True)
-        self.ops(0)[0][1](st.cuda_stream)
-        self.h_sig.copy_(self.sig, non_blocking=True)
-        st.synchronize()
+        Z = self.Z
+        hop, k = self.hop, self.frame_n // self.hop
+        items = []
+        for j, (f0, f1) in enumerate(zip(self.cuts[:-1], self.cuts[1:])):
+            g0 = max(0, f0 - k + 1)
+            last = f1 == self.nf
+            buf = self.slice_sig[j]
+
+            def h2d(st, f0=f0, f1=f1):
+                self.bins[f0:f1].copy_(self.h_bins[f0:f1], non_blocking=True)
+
+            def work(st, g0=g0, f1=f1, buf=buf):
+                self.plan.istft(Z.AOS, self.bins[g0].data_ptr(), None, hop, f1 - g0, buf.data_ptr(),
+                                filter=self.filt.data_ptr(), window=self.win.data_ptr(), stream=st.cuda_stream)
+
+            def d2h(st, f0=f0, f1=f1, g0=g0, buf=buf, last=last):
+                a, b = f0 * hop, (self.total if last else f1 * hop)
+                self.h_sig[a:b].copy_(buf[a - g0 * hop:b - g0 * hop], non_blocking=True)
+            items.append((h2d, work, d2h))
+        self.pipe.run(items)
 
     def cpu_run(self, frames, threads, kind):
         from oracle import oracle as O
