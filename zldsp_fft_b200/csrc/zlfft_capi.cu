@@ -604,12 +604,14 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
     return ZLFFT_OK;
 }
 
-// RFFT<float> of real order 15 (complex order 14) runs as one tile per
-// transform: one pass over HBM with the split fused, against two passes and a
-// split kernel (+18-26% measured, forward, backward and squared magnitudes).
-// The tensor-core form keeps its multi-pass passes.
-bool rfft_tile14(const zlfft_plan_s* p) {
-    return p->cfft_order == 14 && p->kind == ZLFFT_R2C && p->prec == ZLFFT_F32 && !p->tc_form;
+// FP32 complex order 14 (CFFT order 14, RFFT of real order 15) runs as one
+// tile per transform, one pass over HBM. RFFT: the split fused, against two
+// passes and a split kernel (+18-26% measured). CFFT: the next transform's
+// input lands in the exchange buffer while the last group computes (plain
+// +4%, fast form on par with its two passes) and no scratch is needed. The
+// tensor-core form keeps its multi-pass passes.
+bool tile14(const zlfft_plan_s* p) {
+    return p->cfft_order == 14 && p->prec == ZLFFT_F32 && !p->tc_form;
 }
 
 int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,
@@ -671,7 +673,7 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     if (dop == zlfft::kC2RBwd) a.tma = p->use_tma ? 1 : 0;
     const int P = p->cfft_order;
     zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
-    if (P > zlfft::kTileMaxP && !rfft_tile14(p)) {
+    if (P > zlfft::kTileMaxP && !tile14(p)) {
         DeviceGuard g(p->device);
         return exec_multipass(p, dop, in_layout, out_layout, a, stream, ctx);
     }
@@ -1185,7 +1187,7 @@ bool mixed_in_persistent(const MixedGroupHost& g) { return g.P >= zlfft::kMixedM
 int mixed_run_group(zlfft_mixed_s* m, const MixedGroupHost& g, cudaStream_t st) {
     zlfft::LaunchCtx ctx{m->num_sms, &m->launches};
     const zlfft::TileArgs a = mixed_args(m, g);
-    if (g.P > zlfft::kTileMaxP && !rfft_tile14(g.plan))
+    if (g.P > zlfft::kTileMaxP && !tile14(g.plan))
         return exec_multipass(g.plan, g.dop, ZLFFT_AOS, ZLFFT_AOS, a, st, ctx);
     const zlfft::GatherTable& t = g.prec == ZLFFT_F32 ? tables().g32 : tables().g64;
     zlfft::TileLaunchFn fn = t.fn[g.P][g.dop];

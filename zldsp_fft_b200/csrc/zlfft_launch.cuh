@@ -19,10 +19,10 @@ namespace zlfft {
 constexpr int kTileMaxP_f32 = 14;  // tile kernel: whole transform in one CTA
 constexpr int kTileMaxP_f64 = 13;
 constexpr int kTileMaxP = 13;      // orders every path treats as single-CTA
-// FP32 order 14 (128 KB, one CTA per SM) has tile kernels too: the RFFT of
-// real order 15 runs on them from the batched and mixed entry points (one
-// pass over HBM instead of two passes and a split kernel); the CFFT of order
-// 14 measured faster as two passes and stays multi-pass.
+// FP32 order 14 (128 KB, one CTA per SM) has tile kernels too: the CFFT of
+// order 14 and the RFFT of real order 15 run on them from the batched and
+// mixed entry points (one pass over HBM; the other paths keep the multi-pass
+// form).
 constexpr int kTileTableP = 14;
 
 struct LaunchCtx {

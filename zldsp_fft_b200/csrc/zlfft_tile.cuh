@@ -178,7 +178,11 @@ struct TileCfg {
     static constexpr size_t BBYTES = ((size_t)TPC * (N + 1) * sizeof(C) + 15) / 16 * 16;
     static constexpr bool kStageBins = OP == kC2RBwd && sizeof(F) == 4 && (P == 9 || (P >= 11 && P <= 13)) &&
                                        XBYTES + BBYTES <= 200 * 1024;
-    static constexpr size_t SMEM = kTMA ? 2 * XBYTES + 16 : XBYTES + (kStageBins ? BBYTES : 0);
+    // Order-14 CFFT (128 KB: no room for a second buffer): the next tile's
+    // input lands by TMA in the exchange buffer itself, once the last group
+    // has read it, while the last group computes and stores.
+    static constexpr bool kTMA1 = !kTMA && P == 14 && (OP == kC2CFwd || OP == kC2CBwd) && XBYTES + 16 <= 200 * 1024;
+    static constexpr size_t SMEM = kTMA ? 2 * XBYTES + 16 : (kTMA1 ? XBYTES + 16 : XBYTES + (kStageBins ? BBYTES : 0));
     static constexpr int NG = tile_num_groups(P);
     static constexpr int MINB = (65536 / (THREADS * REGS)) > 0 ? (65536 / (THREADS * REGS)) : 1;
 };
@@ -559,7 +563,7 @@ struct TileWorker {
     __device__ __forceinline__ void run(const TileArgs& a, long long tile, bool use_tma, Refill&& refill,
                                         const Sink& sink = Sink{}) {
         static_assert(!Sink::kActive || OP == kC2RBwd, "output sinks take backward RFFT samples");
-        const C* stage = sm + (size_t)TPC * N;
+        const C* stage = Cfg::kTMA1 ? sm : sm + (size_t)TPC * N;
         const long long tr = tile * TPC + slot;
         const bool valid = tr < a.batch;
         // this slot's transform: contiguous (base + stride) or gathered pointers
@@ -712,7 +716,7 @@ struct TileWorker {
                                         v[u * G.R + rho] = kFwd ? x : cswap(x);
                                     }
                                 }
-                                refill();
+                                if constexpr (!Cfg::kTMA1) refill();
                             } else {
                                 constexpr int IL2 = kR2C ? (int)kAoS : IL;
                                 const CxIn<F, IL2> in(ib0, ib1, ibase);
@@ -757,6 +761,9 @@ struct TileWorker {
                                     const C x = sm[ix];
                                     v[u * G.R + rho] = (GI == 0 && OP == kC2RBwd) ? cswap(x) : x;
                                 }
+                            }
+                            if constexpr (kLast && Cfg::kTMA1) {
+                                if (use_tma) refill();  // the buffer is read: the next tile's input may land
                             }
                         }
                         // ---- compute
@@ -919,9 +926,9 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
 
     // ---- TMA staging of each tile's input (one tile ahead)
     constexpr bool kSoAIn = W::kSoAIn;
-    C* stage = reinterpret_cast<C*>(smem_raw) + (size_t)TPC * N;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::XBYTES * 2);
-    const bool use_tma = Cfg::kTMA && !GATHER && a.tma;
+    C* stage = reinterpret_cast<C*>(smem_raw) + (Cfg::kTMA1 ? 0 : (size_t)TPC * N);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::XBYTES * (Cfg::kTMA1 ? 1 : 2));
+    const bool use_tma = (Cfg::kTMA || Cfg::kTMA1) && !GATHER && a.tma;
     auto issue = [&](long long t) {  // warp 0 issues the copies of tile t
         if (!use_tma || threadIdx.x >= 32 || t * TPC >= a.batch) return;
         const long long left = a.batch - t * TPC;
@@ -940,7 +947,7 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
             }
         }
     };
-    if constexpr (Cfg::kTMA) {
+    if constexpr (Cfg::kTMA || Cfg::kTMA1) {
         if (use_tma) {
             if (threadIdx.x == 0) {
                 mbar_init(bar, 1);
@@ -956,7 +963,7 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
     if (use_stage) w.stage_bins(a, blockIdx.x);
 
     for (long long tile = blockIdx.x; tile * TPC < a.batch; tile += gridDim.x) {
-        if constexpr (Cfg::kTMA) {
+        if constexpr (Cfg::kTMA || Cfg::kTMA1) {
             if (use_tma) {
                 const bool ok = mbar_wait(bar, phase);
                 if (__syncthreads_or(!ok)) {  // bounded wait ran out: report and leave
