@@ -178,10 +178,12 @@ struct TileCfg {
     static constexpr size_t BBYTES = ((size_t)TPC * (N + 1) * sizeof(C) + 15) / 16 * 16;
     static constexpr bool kStageBins = OP == kC2RBwd && sizeof(F) == 4 && (P == 9 || (P >= 11 && P <= 13)) &&
                                        XBYTES + BBYTES <= 200 * 1024;
-    // Order-14 CFFT (128 KB: no room for a second buffer): the next tile's
-    // input lands by TMA in the exchange buffer itself, once the last group
-    // has read it, while the last group computes and stores.
-    static constexpr bool kTMA1 = !kTMA && P == 14 && (OP == kC2CFwd || OP == kC2CBwd) && XBYTES + 16 <= 200 * 1024;
+    // 128 KB CFFT tiles (FP32 order 14, FP64 order 13: no room for a second
+    // buffer): the next tile's input lands by TMA in the exchange buffer
+    // itself, once the last group has read it, while the last group computes
+    // and stores.
+    static constexpr bool kTMA1 = !kTMA && (P == 14 || (sizeof(F) == 8 && P == 13)) &&
+                                  (OP == kC2CFwd || OP == kC2CBwd) && XBYTES + 16 <= 200 * 1024;
     static constexpr size_t SMEM = kTMA ? 2 * XBYTES + 16 : (kTMA1 ? XBYTES + 16 : XBYTES + (kStageBins ? BBYTES : 0));
     static constexpr int NG = tile_num_groups(P);
     static constexpr int MINB = (65536 / (THREADS * REGS)) > 0 ? (65536 / (THREADS * REGS)) : 1;
