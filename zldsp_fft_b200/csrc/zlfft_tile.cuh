@@ -178,12 +178,18 @@ struct TileCfg {
     static constexpr size_t BBYTES = ((size_t)TPC * (N + 1) * sizeof(C) + 15) / 16 * 16;
     static constexpr bool kStageBins = OP == kC2RBwd && sizeof(F) == 4 && (P == 9 || (P >= 11 && P <= 13)) &&
                                        XBYTES + BBYTES <= 200 * 1024;
-    // 128 KB CFFT tiles (FP32 order 14, FP64 order 13: no room for a second
+    // 128 KB tiles (FP32 order 14, FP64 order 13: no room for a second
     // buffer): the next tile's input lands by TMA in the exchange buffer
     // itself, once the last group has read it, while the last group computes
-    // and stores.
+    // and stores. For the forward RFFT only where the split runs in registers
+    // (the shuffle epilogue of TileWorker: last group radix 16 = E), so the
+    // buffer is free after the last group's reads.
+    static constexpr int NG_ = tile_num_groups(P);
+    static constexpr Grp GL_ = tile_group(P, NG_ > 0 ? NG_ - 1 : 0);
+    static constexpr bool kShufSplit = (OP == kR2CFwd || OP == kR2CSqrMag) && NG_ >= 2 && GL_.R == E && !GL_.first &&
+                                       GL_.R == 16 && T >= 2;
     static constexpr bool kTMA1 = !kTMA && (P == 14 || (sizeof(F) == 8 && P == 13)) &&
-                                  (OP == kC2CFwd || OP == kC2CBwd) && XBYTES + 16 <= 200 * 1024;
+                                  (OP == kC2CFwd || OP == kC2CBwd || kShufSplit) && XBYTES + 16 <= 200 * 1024;
     static constexpr size_t SMEM = kTMA ? 2 * XBYTES + 16 : (kTMA1 ? XBYTES + 16 : XBYTES + (kStageBins ? BBYTES : 0));
     static constexpr int NG = tile_num_groups(P);
     static constexpr int MINB = (65536 / (THREADS * REGS)) > 0 ? (65536 / (THREADS * REGS)) : 1;
@@ -478,6 +484,7 @@ struct TileWorker {
     static constexpr bool kLastReg = NG >= 2 && GL.R == E && !GL.first && sizeof(F) == 4;
     static constexpr bool kShufPost = kR2C && NG >= 2 && GL.R == E && !GL.first && GL.R == 16 && T >= 2;
     static constexpr int kLastTw = group_tw_count<P, GL.R, GL.L, GL.first>();
+    static_assert(!Cfg::kTMA1 || !kR2C || kShufPost, "single-buffer staging needs the split in registers");
     static constexpr int H = (T < 32 ? T : 32) / 2;  // partner-lane distance of the shuffle split
     static constexpr bool kSoAIn = (IL == kSoA) && !kR2C;
 
