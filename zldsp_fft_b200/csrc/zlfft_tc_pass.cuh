@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256, 3) tc_pass_kernel(const PassArgs a, const
     constexpr int N = Cfg::N, R = Cfg::R, UPC = Cfg::UPC, L_IN = Cfg::L_IN, L_OUT = Cfg::L_OUT, CPT = Cfg::CPT;
     constexpr bool UMAJ = Cfg::kUnitMajorB;
 
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     // first 1024-byte boundary, as an offset into the shared array (keeps the
     // pointer in the shared address space for the compiler)
     unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
