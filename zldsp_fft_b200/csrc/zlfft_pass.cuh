@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                             static_assert(G.R == E, "one radix-16 butterfly per thread");
                             constexpr int ELL = G.L / L_IN;
                             const uint32_t kk = (uint32_t)(ku + L_IN * (tb % ELL));
-                            group16_fast_tw<P, G.L>(kk, static_cast<const C*>(a.tw), fw[GI][0], fw[GI][1]);
+                            group16_fast_tw<P, G.L>(kk, tws, fw[GI][0], fw[GI][1]);
                         }
                     }(),
                     ...);

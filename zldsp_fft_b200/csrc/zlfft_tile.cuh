@@ -422,12 +422,16 @@ __device__ __forceinline__ SplitOut<F> rfft_split(C z1, C z2, F c, F s) {
 // reference's bits.
 //
 // group16_fast_tw loads the two table values; group16_fast_w runs the group
-// from them, so a caller can issue the loads early.
+// from them, so a caller can issue the loads early. Both come from the
+// per-stage tables (stage_l0 layout), where they are contiguous in k:
+// W_{16L}^k is stage 4L's q = 1 entry k and W_{16L}^{4k} = W_{4L}^k is stage
+// L's q = 1 entry k, so consecutive k (lanes) read consecutive entries. (From
+// the unified table they sit 2^s apart, one sector per lane.)
 template <int P, int L, typename C>
-__device__ __forceinline__ void group16_fast_tw(uint32_t k, const C* T, C& w1, C& w4) {
-    constexpr int s = P - ilog2c(16LL * L);  // W_{16L}^{j} = T[j << s], j < 4L < 3N/4 >> s
-    w1 = tw_load(T, k << s);
-    w4 = tw_load(T, (4u * k) << s);
+__device__ __forceinline__ void group16_fast_tw(uint32_t k, const C* tws, C& w1, C& w4) {
+    constexpr uint32_t L0 = (uint32_t)stage_l0(P);
+    w1 = tw_load(tws, 4u * (uint32_t)L - L0 + k);
+    w4 = tw_load(tws, (uint32_t)L - L0 + k);
 }
 
 template <typename C>
@@ -459,9 +463,9 @@ __device__ __forceinline__ void group16_fast_w(C* r, const C w1, const C w4) {
 }
 
 template <int P, int L, typename C>
-__device__ __forceinline__ void group16_fast(C* r, uint32_t k, const C* T) {
+__device__ __forceinline__ void group16_fast(C* r, uint32_t k, const C* tws) {
     C w1, w4;
-    group16_fast_tw<P, L>(k, T, w1, w4);
+    group16_fast_tw<P, L>(k, tws, w1, w4);
     group16_fast_w(r, w1, w4);
 }
 
@@ -519,7 +523,7 @@ struct TileWorker {
                         constexpr bool kLast = (GI + 1 == NG);
                         if constexpr (fast_group<G, kLast>()) {
                             const int b = kLast ? b_last : lt;
-                            group16_fast_tw<P, G.L>((uint32_t)(b % G.L), tw, fw[GI][0], fw[GI][1]);
+                            group16_fast_tw<P, G.L>((uint32_t)(b % G.L), tws, fw[GI][0], fw[GI][1]);
                         }
                     }(),
                     ...);
@@ -785,7 +789,7 @@ struct TileWorker {
                                 if constexpr (fast_group<G, kLast>()) {  // fast-twiddle form, hoisted twiddles
                                     group16_fast_w(v + u * G.R, fw[GI][0], fw[GI][1]);
                                 } else if constexpr (FAST && G.R == 16 && !G.first) {
-                                    group16_fast<P, G.L>(v + u * G.R, (uint32_t)(b % G.L), tw);
+                                    group16_fast<P, G.L>(v + u * G.R, (uint32_t)(b % G.L), tws);
                                 } else {
                                     group_compute_ld<P, G.R, G.L, G.first>(v + u * G.R, (uint32_t)(b % G.L), tws);
                                 }
