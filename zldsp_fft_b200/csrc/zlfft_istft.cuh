@@ -122,12 +122,8 @@ template <typename F, int P, int IL>
 cudaError_t launch_istft(const TileArgs& a, const IstftArgs& o, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = IstftCfg<F, P>;
     auto kern = istft_kernel<F, P, IL>;
-    static const int blocks_per_sm = [kern]() {
-        if (Cfg::SMEM > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, Cfg::T, Cfg::SMEM) != cudaSuccess || b < 1) b = 1;
-        return b;
-    }();
+    static ResidentSlots slots;
+    const int blocks_per_sm = resident_ctas(slots, [kern] { return occupancy_setup(kern, Cfg::T, Cfg::SMEM); });
     if (o.n_frames <= 0 || o.blocks <= 0) return cudaSuccess;
     IstftArgs oo = o;
     const long long cap = (long long)ctx.num_sms * blocks_per_sm;

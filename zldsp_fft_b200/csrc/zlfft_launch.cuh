@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include "zlfft_pass.cuh"
+#include "zlfft_resident.cuh"
 #include "zlfft_tc_pass.cuh"
 #include "zlfft_tile.cuh"
 
@@ -47,16 +48,8 @@ template <typename F, int P, int OP, int IL, int OL, bool WIN = false, bool FAST
 cudaError_t launch_tile(const TileArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = TileCfg<F, P, OP>;
     auto kern = tile_kernel<F, P, OP, IL, OL, false, WIN, FAST>;
-    static const int blocks_per_sm = [kern]() {
-        if (Cfg::SMEM > 48 * 1024) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-        }
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, Cfg::THREADS, Cfg::SMEM) != cudaSuccess || b < 1) {
-            b = 1;
-        }
-        return b;
-    }();
+    static ResidentSlots slots;
+    const int blocks_per_sm = resident_ctas(slots, [kern] { return occupancy_setup(kern, Cfg::THREADS, Cfg::SMEM); });
     if (a.batch <= 0) return cudaSuccess;
     const long long tiles = (a.batch + Cfg::TPC - 1) / Cfg::TPC;
     const long long cap = (long long)ctx.num_sms * blocks_per_sm;
@@ -77,13 +70,8 @@ template <typename F, int P, int OP>
 cudaError_t launch_tile_gather(const TileArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = TileCfg<F, P, OP>;
     auto kern = tile_kernel<F, P, OP, kAoS, kAoS, true>;
-    static const int blocks_per_sm = [kern]() {
-        if (Cfg::SMEM > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, Cfg::THREADS, Cfg::SMEM) != cudaSuccess || b < 1)
-            b = 1;
-        return b;
-    }();
+    static ResidentSlots slots;
+    const int blocks_per_sm = resident_ctas(slots, [kern] { return occupancy_setup(kern, Cfg::THREADS, Cfg::SMEM); });
     if (a.batch <= 0) return cudaSuccess;
     const long long tiles = (a.batch + Cfg::TPC - 1) / Cfg::TPC;
     const long long cap = (long long)ctx.num_sms * blocks_per_sm;
@@ -203,14 +191,8 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
                 a.tma_out = 1;
         }
     }
-    static const int blocks_per_sm = [kern]() {
-        if (Cfg::SMEM > 48 * 1024)
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, Cfg::THREADS, Cfg::SMEM) != cudaSuccess || b < 1)
-            b = 1;
-        return b;
-    }();
+    static ResidentSlots slots;
+    const int blocks_per_sm = resident_ctas(slots, [kern] { return occupancy_setup(kern, Cfg::THREADS, Cfg::SMEM); });
     if (a.batch <= 0) return cudaSuccess;
     const long long items = a.batch * Cfg::CPT;
     const long long cap = (long long)ctx.num_sms * blocks_per_sm;
@@ -330,7 +312,8 @@ cudaError_t launch_tc_pass(const PassArgs& a_in, cudaStream_t stream, const Laun
     // shared memory per CTA (1 KB of it reserved by the driver), with the
     // shared-memory carve-out at its maximum. (The occupancy query answers 1
     // for this kernel, which would leave two thirds of each SM idle.)
-    static const int blocks_per_sm = [kern]() {
+    static ResidentSlots slots;
+    const int blocks_per_sm = resident_ctas(slots, [kern] {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         cudaFuncAttributes fa{};
@@ -346,7 +329,7 @@ cudaError_t launch_tc_pass(const PassArgs& a_in, cudaStream_t stream, const Laun
             if (b < 1) b = 1;
         }
         return b;
-    }();
+    });
     if (a.batch <= 0) return cudaSuccess;
     const long long items = a.batch * Cfg::CPT;
     const long long cap = (long long)ctx.num_sms * blocks_per_sm;

@@ -11,6 +11,7 @@
 // and load-balanced across orders whose costs differ by 2^10.
 #pragma once
 
+#include "zlfft_resident.cuh"
 #include "zlfft_tile.cuh"
 
 namespace zlfft {
@@ -97,12 +98,8 @@ cudaError_t launch_mixed(const MixedGroup* groups, const MixedItem* items, int n
                          cudaStream_t stream, int num_sms) {
     auto kern = mixed_kernel<F>;
     constexpr size_t smem = mixed_smem<F>();
-    static const int blocks_per_sm = [kern]() {
-        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kMixedBlock, smem) != cudaSuccess || b < 1) b = 1;
-        return b;
-    }();
+    static ResidentSlots slots;
+    const int blocks_per_sm = resident_ctas(slots, [kern] { return occupancy_setup(kern, kMixedBlock, smem); });
     if (n_items <= 0) return cudaSuccess;
     const int cap = num_sms * blocks_per_sm;
     kern<<<n_items < cap ? n_items : cap, kMixedBlock, smem, stream>>>(groups, items, n_items, counter);
