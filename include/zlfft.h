@@ -119,7 +119,10 @@ ZLFFT_API int zlfft_exec_host_batched(zlfft_plan plan, int op, int in_layout, in
  * out + b*out_stride + e, strides counted in elements of the buffer's own
  * type (complex for complex buffers, real for real buffers; 0 = dense).
  * Pointers must be aligned to the element type (8 B f32 complex, 16 B f64
- * complex); RFFT real buffers need an even stride. */
+ * complex); RFFT real buffers need an even stride. The multi-pass sizes
+ * (complex order >= 14) pass their intermediates through the plan's scratch,
+ * so calls on one plan must not overlap on the device: issue them on one
+ * stream, order the streams with events, or give each stream its own plan. */
 ZLFFT_API int zlfft_exec_device(zlfft_plan plan, int op, int in_layout, int out_layout, const void* in0, const void* in1,
                       void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, void* stream);
 

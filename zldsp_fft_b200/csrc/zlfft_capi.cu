@@ -280,6 +280,7 @@ struct zlfft_plan_s {
     void* d_in = nullptr;
     void* d_out = nullptr;
     size_t stage_in_bytes = 0, stage_out_bytes = 0;
+    cudaEvent_t ev_host = nullptr;  // orders the chunks' transforms across the two staging streams
     size_t launches = 0;
     // multi-pass scratch (two buffers of `chunk` transforms each)
     void* d_scratch = nullptr;
@@ -326,6 +327,7 @@ void release(zlfft_plan p) {
         if (p->ev_join[i]) cudaEventDestroy(p->ev_join[i]);
     }
     if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+    if (p->ev_host) cudaEventDestroy(p->ev_host);
     if (p->d_in) cudaFree(p->d_in);
     if (p->d_out) cudaFree(p->d_out);
     if (p->h_in) cudaFreeHost(p->h_in);
@@ -969,6 +971,8 @@ int exec_device_noalloc_impl(zlfft_plan_s* p, int op, int in_layout, int out_lay
 }
 
 int ensure_staging(zlfft_plan_s* p, size_t in_bytes, size_t out_bytes) {
+    if (!p->ev_host && cudaEventCreateWithFlags(&p->ev_host, cudaEventDisableTiming) != cudaSuccess)
+        return fail(ZLFFT_ERR_CUDA, "event creation failed");
     if (in_bytes > p->stage_in_bytes) {
         if (p->h_in) cudaFreeHost(p->h_in);
         if (p->d_in) cudaFree(p->d_in);
@@ -1038,26 +1042,41 @@ int exec_host_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const
     size_t chunk = (16u << 20) / (in_part * in_parts);
     if (chunk == 0) chunk = 1;
     if (chunk > batch) chunk = batch;
+    // The chunks' copies alternate between two streams. Their transforms share
+    // the plan's scratch (orders >= 14), so each one waits for the previous
+    // chunk's (ev_host); the copies still overlap the neighbouring transforms.
     cudaStream_t ss[2] = {p->stream, p->stream2};
+    // on failure, let every copy already queued finish before returning, so
+    // nothing touches the caller's buffers afterwards
+    auto drain = [&](int code) {
+        cudaStreamSynchronize(ss[0]);
+        cudaStreamSynchronize(ss[1]);
+        return code;
+    };
     for (size_t b0 = 0, c = 0; b0 < batch; b0 += chunk, ++c) {
         const size_t nb = (batch - b0 < chunk) ? batch - b0 : chunk;
         cudaStream_t st = ss[c & 1];
         for (int q = 0; q < in_parts; ++q) {
             const char* h = pin_in ? static_cast<const char*>(src[q]) : static_cast<const char*>(p->h_in) + q * in_part * batch;
-            ZL_CUDA(cudaMemcpyAsync(din + q * in_part * batch + b0 * in_part, h + b0 * in_part, nb * in_part,
-                                    cudaMemcpyHostToDevice, st));
+            const cudaError_t e = cudaMemcpyAsync(din + q * in_part * batch + b0 * in_part, h + b0 * in_part,
+                                                  nb * in_part, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return drain(cuda_fail(e, "cudaMemcpyAsync (H2D)"));
         }
         const void* i0 = din + b0 * in_part;
         const void* i1 = in_soa ? din + in_part * batch + b0 * in_part : nullptr;
         void* o0 = dout + b0 * out_part;
         void* o1 = out_soa ? dout + out_part * batch + b0 * out_part : nullptr;
+        if (c > 0 && cudaStreamWaitEvent(st, p->ev_host, 0) != cudaSuccess)
+            return drain(fail(ZLFFT_ERR_CUDA, "stream wait failed"));
         // dense strides: the device buffers hold whole transforms back to back
         rc = exec_device_impl(p, op, in_layout, out_layout, i0, i1, o0, o1, nb, 0, 0, st);
-        if (rc) return rc;
+        if (rc) return drain(rc);
+        if (cudaEventRecord(p->ev_host, st) != cudaSuccess) return drain(fail(ZLFFT_ERR_CUDA, "event record failed"));
         for (int q = 0; q < out_parts; ++q) {
             char* h = pin_out ? static_cast<char*>(dst[q]) : static_cast<char*>(p->h_out) + q * out_part * batch;
-            ZL_CUDA(cudaMemcpyAsync(h + b0 * out_part, dout + q * out_part * batch + b0 * out_part, nb * out_part,
-                                    cudaMemcpyDeviceToHost, st));
+            const cudaError_t e = cudaMemcpyAsync(h + b0 * out_part, dout + q * out_part * batch + b0 * out_part,
+                                                  nb * out_part, cudaMemcpyDeviceToHost, st);
+            if (e != cudaSuccess) return drain(cuda_fail(e, "cudaMemcpyAsync (D2H)"));
         }
     }
     ZL_CUDA(cudaStreamSynchronize(ss[0]));
