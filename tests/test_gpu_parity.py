@@ -411,3 +411,68 @@ def test_host_batched_multichunk_equals_device(case):
         plan.exec_host(op, Z.AOS, Z.AOS, hin.data_ptr(), None, hout.data_ptr(), None, b)
         assert np.array_equal(hout.numpy().view(out.dtype).reshape(out.shape), ref), case
     assert plan.device_status() == 0
+
+
+
+def test_threads_share_plans():
+    """Host threads share plans: two call one order-16 plan through the
+    host-batched path (serialised on the plan's staging lock), and two call
+    one order-12 plan (single-CTA tiles, no scratch) through the device path
+    on their own streams, all at once. Every result equals the
+    single-threaded one, and each plan's launch counter (atomic) counts every
+    launch."""
+    import threading
+    import torch
+    rng = np.random.default_rng(31)
+    big, small = Z.Plan(Z.C2C, 16, np.float32), Z.Plan(Z.C2C, 12, np.float32)
+    xb = [(rng.uniform(-1, 1, (64, 1 << 16)) + 1j * rng.uniform(-1, 1, (64, 1 << 16))).astype(np.complex64)
+          for _ in range(2)]
+    xs = [(rng.uniform(-1, 1, (512, 1 << 12)) + 1j * rng.uniform(-1, 1, (512, 1 << 12))).astype(np.complex64)
+          for _ in range(2)]
+    rb = [G.run_c2c(big, x, True) for x in xb]
+    rs = [G.run_c2c(small, x, True) for x in xs]
+    # launches of one call on each path, measured alone
+    ob = np.zeros_like(xb[0])
+    big.take_launch_count()
+    big.exec_host(Z.FORWARD, Z.AOS, Z.AOS, xb[0].ctypes.data, None, ob.ctypes.data, None, 64)
+    per_host = big.take_launch_count()
+    small.take_launch_count()
+    G.run_c2c(small, xs[0], True)
+    per_dev = small.take_launch_count()
+    reps, errors = 3, []
+    tin = [G.dev(x) for x in xs]
+    tout = [torch.zeros((512, 1 << 12, 2), dtype=torch.float32, device="cuda") for _ in xs]
+    streams = [torch.cuda.Stream() for _ in xs]
+
+    def host_worker(i):
+        try:
+            out = np.zeros_like(xb[i])
+            for _ in range(reps):
+                big.exec_host(Z.FORWARD, Z.AOS, Z.AOS, xb[i].ctypes.data, None, out.ctypes.data, None, 64)
+                if not np.array_equal(out, rb[i]):
+                    errors.append(("host", i))
+        except Exception as e:  # noqa: BLE001 - reported by the assertion below
+            errors.append(("host", i, repr(e)))
+
+    def device_worker(i):
+        try:
+            for _ in range(reps):
+                small.exec_device(Z.FORWARD, Z.AOS, Z.AOS, tin[i].data_ptr(), None, tout[i].data_ptr(), None, 512,
+                                  stream=streams[i].cuda_stream)
+                streams[i].synchronize()
+                o = G.host(tout[i])
+                if not np.array_equal((o[..., 0] + 1j * o[..., 1]).astype(np.complex64), rs[i]):
+                    errors.append(("device", i))
+        except Exception as e:  # noqa: BLE001 - reported by the assertion below
+            errors.append(("device", i, repr(e)))
+
+    ths = [threading.Thread(target=host_worker, args=(i,)) for i in range(2)]
+    ths += [threading.Thread(target=device_worker, args=(i,)) for i in range(2)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    assert not errors, errors
+    assert big.take_launch_count() == 2 * reps * per_host
+    assert small.take_launch_count() == 2 * reps * per_dev
+    assert big.device_status() == 0 and small.device_status() == 0

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -281,7 +282,7 @@ struct zlfft_plan_s {
     void* d_out = nullptr;
     size_t stage_in_bytes = 0, stage_out_bytes = 0;
     cudaEvent_t ev_host = nullptr;  // orders the chunks' transforms across the two staging streams
-    size_t launches = 0;
+    std::atomic<size_t> launches{0};
     // multi-pass scratch (two buffers of `chunk` transforms each)
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -297,7 +298,8 @@ struct zlfft_plan_s {
     bool fast_form = false; // multi-pass radix-16 groups with fast twiddles (ZLFFT_MODE_FAST)
     bool fuse_split = false;  // RFFT forward: split fused into the last pass (else its own kernel)
     int store_tma = -1;       // first pass output by TMA tensor stores (-1: the precision's default)
-    std::mutex mu;
+    std::mutex mu;            // the host path's staging buffers and streams
+    std::mutex scratch_mu;    // first-use creation of the scratch, lanes and their events
 };
 
 namespace {
@@ -374,6 +376,7 @@ bool aligned(const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(pt
 // chunk is sized so that one chunk's intermediates (both buffers) stay in
 // L2 between the passes; it is reused chunk after chunk.
 int ensure_scratch(zlfft_plan_s* p) {
+    std::lock_guard<std::mutex> lock(p->scratch_mu);
     if (p->d_scratch) return ZLFFT_OK;
     const size_t cx = 2 * p->esize;
     const size_t n = size_t{1} << p->cfft_order;
@@ -385,20 +388,28 @@ int ensure_scratch(zlfft_plan_s* p) {
     }
     size_t chunk = budget / per;
     if (chunk == 0) chunk = 1;
+    // the streams and events first: d_scratch is set last, so a failure
+    // leaves the plan as it was and a later call tries again
+    for (int i = 0; i < 2; ++i) {
+        if ((!p->lanes[i] && cudaStreamCreateWithFlags(&p->lanes[i], cudaStreamNonBlocking) != cudaSuccess) ||
+            (!p->ev_join[i] && cudaEventCreateWithFlags(&p->ev_join[i], cudaEventDisableTiming) != cudaSuccess)) {
+            cudaGetLastError();
+            return fail(ZLFFT_ERR_CUDA, "stream creation failed");
+        }
+    }
+    if (!p->ev_fork && cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ZLFFT_ERR_CUDA, "event creation failed");
+    }
     const size_t bytes = 4 * chunk * per;  // two buffers for each of the two chunk pipelines
-    if (cudaMalloc(&p->d_scratch, bytes) != cudaSuccess) {
+    void* d = nullptr;
+    if (cudaMalloc(&d, bytes) != cudaSuccess) {
         cudaGetLastError();
         return fail(ZLFFT_ERR_ALLOC, "scratch allocation of %zu bytes failed", bytes);
     }
     p->scratch_bytes = bytes;
     p->chunk = chunk;
-    for (int i = 0; i < 2; ++i) {
-        if (cudaStreamCreateWithFlags(&p->lanes[i], cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&p->ev_join[i], cudaEventDisableTiming) != cudaSuccess)
-            return fail(ZLFFT_ERR_CUDA, "stream creation failed");
-    }
-    if (cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) != cudaSuccess)
-        return fail(ZLFFT_ERR_CUDA, "event creation failed");
+    p->d_scratch = d;
     return ZLFFT_OK;
 }
 
@@ -1138,7 +1149,7 @@ struct zlfft_mixed_s {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     size_t graph_launches = 0;  // kernels recorded in the graph
-    size_t launches = 0;
+    std::atomic<size_t> launches{0};
     std::mutex mu;
 };
 
@@ -1658,8 +1669,7 @@ int zlfft_exec_device_noalloc(zlfft_plan plan, int op, int in_layout, int out_la
 
 int zlfft_plan_take_launch_count(zlfft_plan plan, size_t* launches) {
     if (!plan || !launches) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
-    *launches = plan->launches;
-    plan->launches = 0;
+    *launches = plan->launches.exchange(0);
     return ZLFFT_OK;
 }
 
@@ -1714,8 +1724,7 @@ int zlfft_mixed_exec(zlfft_mixed mixed, int schedule, void* stream) {
 int zlfft_mixed_take_launch_count(zlfft_mixed mixed, size_t* launches) {
     if (!mixed || !launches) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
     std::lock_guard<std::mutex> lock(mixed->mu);
-    *launches = mixed->launches;
-    mixed->launches = 0;
+    *launches = mixed->launches.exchange(0);
     return ZLFFT_OK;
 }
 

@@ -10,6 +10,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
+
 #include "zlfft_pass.cuh"
 #include "zlfft_resident.cuh"
 #include "zlfft_tc_pass.cuh"
@@ -28,7 +30,7 @@ constexpr int kTileTableP = 14;
 
 struct LaunchCtx {
     int num_sms;
-    size_t* launches;  // incremented per kernel launch
+    std::atomic<size_t>* launches;  // incremented per kernel launch
 };
 
 using TileLaunchFn = cudaError_t (*)(const TileArgs&, cudaStream_t, const LaunchCtx&);
