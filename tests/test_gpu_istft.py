@@ -142,3 +142,39 @@ def test_istft_errors():
     with pytest.raises(Z.ZlfftError):  # a CFFT plan
         Z.Plan(Z.C2C, 12, np.float32).istft(Z.AOS, b.data_ptr(), None, 1024, 4, s.data_ptr())
     p.istft(Z.AOS, b.data_ptr(), None, 1024, 0, s.data_ptr())  # no frames: nothing to do
+
+
+@pytest.mark.parametrize("order,hop,nf,slices", [(12, 1024, 1021, 8), (10, 128, 300, 7), (11, 2048, 50, 4),
+                                                 (12, 512, 40, 13)])
+def test_istft_slices_reassemble_bit_exact(order, hop, nf, slices):
+    """Host-copy pipelining: slice [f0, f1) launched on frames
+    [f0 - K + 1, f1) into its own buffer holds final sums for its blocks
+    [f0, f1) (plus the tail, for the last slice). Copying only those back
+    rebuilds the single launch's signal bit for bit, whatever the cuts."""
+    import torch
+    n = 1 << order
+    k = n // hop
+    rng = np.random.default_rng(1500 + order + hop)
+    X = _bins(rng, nf, n, np.complex64)
+    H = _bins(rng, 1, n, np.complex64)[0]
+    win = _hann(n, np.float32)
+    plan = Z.Plan(Z.R2C, order, np.float32)
+    whole = _run(plan, X, hop, H, win)
+    host = np.zeros((nf, n // 2 + 1, 2), np.float32)
+    host[..., 0], host[..., 1] = X.real, X.imag
+    tb = torch.from_numpy(host).cuda()
+    th = torch.from_numpy(np.stack([H.real, H.imag], -1).astype(np.float32)).cuda()
+    tw = torch.from_numpy(win).cuda()
+    total = (nf - 1) * hop + n
+    out = np.full(total, np.nan, np.float32)
+    cuts = sorted(set([0, nf] + list(rng.integers(1, nf, slices - 1))))
+    for f0, f1 in zip(cuts[:-1], cuts[1:]):
+        g0 = max(0, f0 - k + 1)
+        buf = torch.full(((f1 - g0 - 1) * hop + n,), float("nan"), dtype=torch.float32, device="cuda")
+        plan.istft(Z.AOS, tb[g0].data_ptr(), None, hop, f1 - g0, buf.data_ptr(), filter=th.data_ptr(),
+                   window=tw.data_ptr())
+        torch.cuda.synchronize()
+        a, b = f0 * hop, (total if f1 == nf else f1 * hop)
+        out[a:b] = buf[a - g0 * hop:b - g0 * hop].cpu().numpy()
+    assert plan.device_status() == 0
+    assert np.array_equal(out, whole), (order, hop, cuts)
