@@ -119,7 +119,11 @@ ZLFFT_API int zlfft_exec_host_batched(zlfft_plan plan, int op, int in_layout, in
  * out + b*out_stride + e, strides counted in elements of the buffer's own
  * type (complex for complex buffers, real for real buffers; 0 = dense).
  * Pointers must be aligned to the element type (8 B f32 complex, 16 B f64
- * complex); RFFT real buffers need an even stride. The multi-pass sizes
+ * complex); RFFT real buffers need an even stride. In place: an output may
+ * share memory with an input only from the same start with the same byte
+ * stride (CFFT with equal strides; RFFT with real stride 2*(N/2+1), the
+ * padded layout); other overlaps with batch > 1 are refused
+ * (ZLFFT_ERR_INVALID_ARG). The multi-pass sizes
  * (complex order >= 14) pass their intermediates through the plan's scratch,
  * so calls on one plan must not overlap on the device: issue them on one
  * stream, order the streams with events, or give each stream its own plan. */

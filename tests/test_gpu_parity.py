@@ -476,3 +476,42 @@ def test_threads_share_plans():
     assert big.take_launch_count() == 2 * reps * per_host
     assert small.take_launch_count() == 2 * reps * per_dev
     assert big.device_status() == 0 and small.device_status() == 0
+
+
+def test_padded_in_place_rfft_and_cross_transform_aliasing_refused():
+    """The padded in-place RFFT (real stride N + 2 = two reals per bin, same
+    start and byte stride as the bins) runs forward and backward on the tile
+    and multi-pass paths, equal to the out-of-place results bit for bit.
+    Overlaps that would let one transform's output overwrite another's input
+    (dense in place RFFT, in place with different strides, a shifted output)
+    are refused."""
+    import torch
+    for order in (12, 16):  # single-CTA tiles; multi-pass
+        n, nb = 1 << order, (1 << order) // 2 + 1
+        plan = Z.Plan(Z.R2C, order, np.float32)
+        rng = np.random.default_rng(60 + order)
+        b = 6
+        x = rng.uniform(-1, 1, (b, n)).astype(np.float32)
+        ref = G.run_r2c(plan, x)
+        buf = torch.zeros((b, 2 * nb), dtype=torch.float32, device="cuda")
+        buf[:, :n] = torch.from_numpy(x).cuda()
+        plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, buf.data_ptr(), None, buf.data_ptr(), None, b, 2 * nb, nb)
+        torch.cuda.synchronize()
+        got = G.host(buf).reshape(b, nb, 2)
+        assert np.array_equal(got[..., 0] + 1j * got[..., 1], ref), order
+        back_ref = G.run_c2r(plan, ref)
+        plan.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, buf.data_ptr(), None, buf.data_ptr(), None, b, nb, 2 * nb)
+        torch.cuda.synchronize()
+        assert np.array_equal(G.host(buf)[:, :n], back_ref), order
+        with pytest.raises(Z.ZlfftError) as e:  # dense: real stride N, bin stride N/2 + 1
+            plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, buf.data_ptr(), None, buf.data_ptr(), None, b, n, nb)
+        assert e.value.code == Z._capi.ERR_INVALID_ARG
+        assert plan.device_status() == 0
+    cplan = Z.Plan(Z.C2C, 9, np.float32)
+    t = torch.zeros((8, 512, 2), dtype=torch.float32, device="cuda")
+    with pytest.raises(Z.ZlfftError) as e:
+        cplan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, t.data_ptr(), None, t.data_ptr(), None, 4, 512, 520)
+    assert e.value.code == Z._capi.ERR_INVALID_ARG
+    with pytest.raises(Z.ZlfftError) as e:
+        cplan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, t.data_ptr(), None, t[1].data_ptr(), None, 4)
+    assert e.value.code == Z._capi.ERR_INVALID_ARG

@@ -372,6 +372,44 @@ int device_op_code(const zlfft_plan_s* p, int op) {
 
 bool aligned(const void* ptr, size_t a) { return (reinterpret_cast<uintptr_t>(ptr) % a) == 0; }
 
+// Aliasing of a batched call. Every kernel reads a transform's whole input
+// before it writes that transform's output, and transforms are disjoint, so
+// an output may share memory with an input when both start at the same
+// address with the same byte stride (in-place CFFT; the padded in-place RFFT
+// whose real stride is 2 * (N/2 + 1)): each transform then overwrites only
+// its own input. Any other overlap, with more than one transform, lets one
+// transform's output overwrite another's input before it is read.
+int check_aliasing(const zlfft_plan_s* p, const Extents& ex, bool in_soa, bool out_soa, const void* in0,
+                   const void* in1, const void* out0, const void* out1, size_t batch, size_t in_stride,
+                   size_t out_stride) {
+    if (batch <= 1) return ZLFFT_OK;
+    struct Span {
+        uintptr_t lo, hi;
+        size_t step;  // bytes from one transform to the next
+    };
+    auto span = [&](const void* ptr, size_t unit, size_t elems, size_t stride) {
+        const uintptr_t lo = reinterpret_cast<uintptr_t>(ptr);
+        return Span{lo, lo + ((batch - 1) * stride + elems) * unit, stride * unit};
+    };
+    const size_t in_unit = ex.in_complex && !in_soa ? 2 * p->esize : p->esize;
+    const size_t out_unit = ex.out_complex && !out_soa ? 2 * p->esize : p->esize;
+    Span ins[2], outs[2];
+    int ni = 0, no = 0;
+    ins[ni++] = span(in0, in_unit, ex.in_elems, in_stride);
+    if (in_soa) ins[ni++] = span(in1, in_unit, ex.in_elems, in_stride);
+    outs[no++] = span(out0, out_unit, ex.out_elems, out_stride);
+    if (out_soa) outs[no++] = span(out1, out_unit, ex.out_elems, out_stride);
+    for (int i = 0; i < ni; ++i)
+        for (int o = 0; o < no; ++o) {
+            const Span& a = ins[i];
+            const Span& b = outs[o];
+            if (a.lo < b.hi && b.lo < a.hi && !(a.lo == b.lo && a.step == b.step))
+                return fail(ZLFFT_ERR_INVALID_ARG,
+                            "input and output overlap across transforms (in place needs the same start and byte stride)");
+        }
+    return ZLFFT_OK;
+}
+
 // Scratch for the multi-pass orders: two buffers of `chunk` transforms. The
 // chunk is sized so that one chunk's intermediates (both buffers) stay in
 // L2 between the passes; it is reused chunk after chunk.
@@ -656,6 +694,8 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
         return fail(ZLFFT_ERR_INVALID_ARG, "RFFT real output stride must be even");
     if (p->kind == ZLFFT_C2C && in0 == out0 && in_layout != out_layout)
         return fail(ZLFFT_ERR_INVALID_ARG, "in-place transform needs the same layout on both sides");
+    rc = check_aliasing(p, ex, in_soa, out_soa, in0, in1, out0, out1, batch, in_stride, out_stride);
+    if (rc) return rc;
     if (batch == 0) return ZLFFT_OK;
 
     zlfft::TileArgs a{};
@@ -967,6 +1007,8 @@ int exec_device_noalloc_impl(zlfft_plan_s* p, int op, int in_layout, int out_lay
         return fail(ZLFFT_ERR_INVALID_ARG, "RFFT real output stride must be even");
     if (p->kind == ZLFFT_C2C && in0 == out0 && in_layout != out_layout)
         return fail(ZLFFT_ERR_INVALID_ARG, "in-place transform needs the same layout on both sides");
+    rc = check_aliasing(p, ex, in_soa, out_soa, in0, in1, out0, out1, batch, in_stride, out_stride);
+    if (rc) return rc;
     if (batch == 0) return ZLFFT_OK;
     zlfft::TileArgs a{};
     a.in0 = in0;
