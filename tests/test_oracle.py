@@ -162,3 +162,29 @@ def test_istft_port_overlap_add(oracle):
         ref = oracle.istft_fp64(X, hop, H, win)
         assert y.shape == ((nf - 1) * hop + n,)
         assert np.linalg.norm(y - ref) / np.linalg.norm(ref) <= (n // hop) * oracle.tolerance(order, "f32")
+
+
+def test_istft_slicing_recipe_on_the_oracle(oracle):
+    """The slicing recipe for pipelining host copies with the inverse STFT,
+    on the oracle's sequential overlap-add: slice [f0, f1) runs frames
+    [max(0, f0 - K + 1), f1) into its own signal; its samples
+    [f0 * hop, f1 * hop) (to the end, for the last slice) are final and,
+    reassembled, equal one run over all frames bit for bit."""
+    rng = np.random.default_rng(1502)
+    order, nf = 8, 37
+    n = 1 << order
+    X = (rng.uniform(-1, 1, (nf, n // 2 + 1)) + 1j * rng.uniform(-1, 1, (nf, n // 2 + 1))).astype(np.complex64)
+    X[:, 0], X[:, -1] = X[:, 0].real, X[:, -1].real
+    win = (0.5 - 0.5 * np.cos(2 * np.pi * np.arange(n) / n)).astype(np.float32)
+    for hop in (n, n // 4, n // 8):
+        k = n // hop
+        whole = oracle.istft_port(X, hop, X[1], win)
+        total = (nf - 1) * hop + n
+        for cuts in ([0, nf], [0, 1, 2, nf], [0, 5, 6, 20, 33, nf], list(range(nf + 1))):
+            out = np.full(total, np.nan, np.float32)
+            for f0, f1 in zip(cuts[:-1], cuts[1:]):
+                g0 = max(0, f0 - k + 1)
+                part = oracle.istft_port(X[g0:f1], hop, X[1], win)
+                a, b = f0 * hop, (total if f1 == nf else f1 * hop)
+                out[a:b] = part[a - g0 * hop:b - g0 * hop]
+            assert np.array_equal(out, whole), (hop, cuts)
