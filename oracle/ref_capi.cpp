@@ -4,7 +4,7 @@
 // shim (oracle/hwy_shim). The build recipe (oracle/Makefile) points -I at the
 // reference's own src/ directory; no reference source is copied.
 //
-// Used by the tests as a parity checker and by bench.py as the timed CPU
+// Used by the tests to check parity and by bench.py as the timed CPU
 // baseline. Never linked into the product library.
 //
 // Batch conventions (all pointers host memory):

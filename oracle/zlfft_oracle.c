@@ -5,7 +5,7 @@
  * execute.hpp:318-536). Each function cites the reference lines it follows.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
- * load this library, and only as the checker or the timed CPU baseline. The
+ * load this library, and only to check results or as the timed CPU baseline. The
  * product (libzlfft_cuda.so) never calls it.
  *
  * Rounding follows the reference: every MulAdd / NegMulAdd of the reference

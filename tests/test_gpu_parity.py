@@ -1,7 +1,7 @@
 """GPU parity: the CUDA kernels, called through the C ABI on device buffers,
 against the oracle on the same seeded inputs.
 
-Tolerance (north star): relative L2 <= 4*log2(N)*eps against the FP64 oracle
+Tolerance: relative L2 <= 4*log2(N)*eps against the FP64 oracle
 (eps = 2^-24 f32, 2^-53 f64). The plain form rebuilds the reference's own
 arithmetic, so in f32 (where the device-generated twiddle table is bit-equal
 to the reference's) the output must also be BIT-IDENTICAL to the oracle's C

@@ -1,7 +1,7 @@
 // G7: one persistent launch for a mixed batch of transforms of many orders.
 //
-// A mixed batch (the north star's "thousands of transforms of uneven order,
-// CFFT and RFFT mixed") is grouped on the host by (kind, order, operation);
+// A mixed batch (thousands of transforms of uneven order, CFFT and RFFT
+// mixed) is grouped on the host by (kind, order, operation);
 // each group is cut into tiles of the tile kernel's shape (TPC transforms of
 // one order, 128 threads). All tiles of all groups with orders that fit a
 // 128-thread CTA (complex orders <= 11) form one work list, sorted longest
