@@ -254,7 +254,10 @@ typedef struct zlfft_mixed_s* zlfft_mixed;
  * persistent kernel's work list (tiles sorted longest first) and the
  * multi-pass intermediates, all allocated here, so that zlfft_mixed_exec
  * allocates nothing and may be recorded into a CUDA graph. The descriptors
- * are copied; the buffers they point to are used by every exec. */
+ * are copied; the buffers they point to are used by every exec. The
+ * transforms run concurrently, so an output must not overlap another
+ * descriptor's output or input (ZLFFT_ERR_INVALID_ARG); inputs may be shared,
+ * and out == in runs a transform in place. */
 ZLFFT_API int zlfft_mixed_create(zlfft_mixed* mixed, const zlfft_desc* descs, size_t n, int device);
 
 /* Run every transform of the batch on `stream` (a cudaStream_t; NULL = the

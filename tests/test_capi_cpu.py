@@ -83,6 +83,42 @@ def test_mixed_batch_descriptors_rejected_without_cuda():
     assert lib.zlfft_mixed_destroy(None) == C.OK
 
 
+def test_mixed_batch_overlaps_rejected_without_cuda():
+    """The transforms of a mixed batch run concurrently, so zlfft_mixed_create
+    refuses outputs that overlap another transform's output or input (checked
+    before it touches CUDA). Shared inputs and in place are accepted."""
+    lib = C.lib()
+    h = ctypes.c_void_p()
+    mib = 1 << 20
+    n10 = 8 << 10  # bytes of a CFFT<float> of order 10
+
+    def create(*descs):
+        arr = (C.Desc * len(descs))(*[C.Desc(kind=k, precision=C.F32, order=o, op=op, in_=i, out=out)
+                                      for k, o, op, i, out in descs])
+        rc = lib.zlfft_mixed_create(ctypes.byref(h), arr, len(descs), -1)
+        if rc == C.OK:  # a GPU is present: the batch was built
+            lib.zlfft_mixed_destroy(h)
+        return rc
+
+    a = (C.C2C, 10, C.FORWARD, 1 * mib, 2 * mib)
+    # outputs overlap
+    assert create(a, (C.C2C, 10, C.FORWARD, 3 * mib, 2 * mib + n10 - 8)) == C.ERR_INVALID_ARG
+    assert "outputs overlap" in C.last_error()
+    # the second transform reads the first one's output; the first overwrites the second's input in place
+    assert create(a, (C.C2C, 10, C.FORWARD, 2 * mib, 4 * mib)) == C.ERR_INVALID_ARG
+    assert "writes over the input" in C.last_error()
+    assert create((C.C2C, 10, C.FORWARD, 1 * mib, 1 * mib), (C.C2C, 9, C.BACKWARD, 1 * mib + 64, 4 * mib)) \
+        == C.ERR_INVALID_ARG
+    # an RFFT forward output (N/2 + 1 bins) runs 8 bytes past its input into the next transform's input
+    assert create((C.R2C, 10, C.FORWARD, 1 * mib, 1 * mib), (C.C2C, 4, C.FORWARD, 1 * mib + 4096, 4 * mib)) \
+        == C.ERR_INVALID_ARG
+    # accepted (then CUDA is needed): shared inputs, in place, a forward_sqr_mag output packed right
+    # after another transform's
+    ok = create(a, (C.C2C, 10, C.BACKWARD, 1 * mib, 3 * mib), (C.C2C, 8, C.FORWARD, 5 * mib, 5 * mib),
+                (C.R2C, 10, C.FORWARD_SQR_MAG, 6 * mib, 2 * mib + n10))
+    assert ok in (C.ERR_CUDA, C.OK), C.last_error()
+
+
 def test_python_mirror_rejects_bad_buffers():
     from zldsp_fft_b200.fft import _complex_arg, _real_arg
     import numpy as np

@@ -1236,6 +1236,56 @@ int mixed_validate(const zlfft_desc& d, size_t i) {
     return ZLFFT_OK;
 }
 
+// The transforms of a mixed batch run concurrently, in no fixed order. So no
+// output may overlap another transform's output or input: the result would
+// depend on the schedule, where the reference's calls, one after another,
+// have one answer. Inputs may be shared, and a transform's output may overlap
+// its own input (every kernel reads a transform's input before writing its
+// output), which covers in place. O(n log n): outputs sorted by start must be
+// disjoint; each input is then checked against the outputs around it.
+int mixed_check_overlaps(const zlfft_desc* descs, size_t n) {
+    struct Span {
+        uintptr_t lo, hi;
+        size_t i;
+    };
+    std::vector<Span> outs(n), ins(n);
+    for (size_t i = 0; i < n; ++i) {
+        const zlfft_desc& d = descs[i];
+        const size_t es = d.precision == ZLFFT_F32 ? 4 : 8;
+        const size_t N = size_t{1} << d.order, nb = N / 2 + 1;
+        size_t ib, ob;
+        if (d.kind == ZLFFT_C2C) {
+            ib = ob = 2 * es * N;
+        } else if (d.op == ZLFFT_BACKWARD) {
+            ib = 2 * es * nb;
+            ob = es * N;
+        } else {
+            ib = es * N;
+            ob = d.op == ZLFFT_FORWARD ? 2 * es * nb : es * nb;
+        }
+        const uintptr_t in = reinterpret_cast<uintptr_t>(d.in), out = reinterpret_cast<uintptr_t>(d.out);
+        ins[i] = Span{in, in + ib, i};
+        outs[i] = Span{out, out + ob, i};
+    }
+    std::sort(outs.begin(), outs.end(), [](const Span& a, const Span& b) { return a.lo < b.lo; });
+    for (size_t k = 0; k + 1 < n; ++k)
+        if (outs[k].hi > outs[k + 1].lo)
+            return fail(ZLFFT_ERR_INVALID_ARG,
+                        "descriptors %zu and %zu: outputs overlap (the transforms of a batch run concurrently)",
+                        outs[k].i, outs[k + 1].i);
+    for (const Span& a : ins) {
+        // outputs are disjoint and sorted, so their ends are sorted too
+        auto it = std::upper_bound(outs.begin(), outs.end(), a.lo, [](uintptr_t v, const Span& o) { return v < o.hi; });
+        for (; it != outs.end() && it->lo < a.hi; ++it)
+            if (it->i != a.i)
+                return fail(ZLFFT_ERR_INVALID_ARG,
+                            "descriptor %zu writes over the input of descriptor %zu (the transforms of a batch run "
+                            "concurrently)",
+                            it->i, a.i);
+    }
+    return ZLFFT_OK;
+}
+
 // Cost of one persistent tile of complex order P (points x stages): orders
 // 4 and up hold 128 * 16 points per tile, so the cost grows with P.
 long long mixed_tile_cost(int P) { return (long long)zlfft::mixed_tpc(P) * (1LL << P) * (P > 0 ? P : 1); }
@@ -1328,6 +1378,7 @@ int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int d
         int rc = mixed_validate(descs[i], i);
         if (rc) return rc;
     }
+    if (int rc = mixed_check_overlaps(descs, n)) return rc;
     if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return fail(ZLFFT_ERR_CUDA, "no CUDA device");
     auto* m = new zlfft_mixed_s();
     m->device = device;
