@@ -37,8 +37,17 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
+// A failed runtime call leaves its error pending for the next
+// cudaGetLastError(), which would then report it against a later, successful
+// launch; the failure paths below clear it once they have recorded it.
 int cuda_fail(cudaError_t e, const char* what) {
+    cudaGetLastError();
     return fail(ZLFFT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int alloc_fail(const char* what, size_t bytes) {
+    cudaGetLastError();
+    return fail(ZLFFT_ERR_ALLOC, "%s allocation of %zu bytes failed", what, bytes);
 }
 
 #define ZL_CUDA(call)                                  \
@@ -1032,7 +1041,7 @@ int ensure_staging(zlfft_plan_s* p, size_t in_bytes, size_t out_bytes) {
         p->h_in = p->d_in = nullptr;
         p->stage_in_bytes = 0;
         if (cudaMallocHost(&p->h_in, in_bytes) != cudaSuccess || cudaMalloc(&p->d_in, in_bytes) != cudaSuccess)
-            return fail(ZLFFT_ERR_ALLOC, "staging allocation of %zu bytes failed", in_bytes);
+            return alloc_fail("staging", in_bytes);
         p->stage_in_bytes = in_bytes;
     }
     if (out_bytes > p->stage_out_bytes) {
@@ -1041,7 +1050,7 @@ int ensure_staging(zlfft_plan_s* p, size_t in_bytes, size_t out_bytes) {
         p->h_out = p->d_out = nullptr;
         p->stage_out_bytes = 0;
         if (cudaMallocHost(&p->h_out, out_bytes) != cudaSuccess || cudaMalloc(&p->d_out, out_bytes) != cudaSuccess)
-            return fail(ZLFFT_ERR_ALLOC, "staging allocation of %zu bytes failed", out_bytes);
+            return alloc_fail("staging", out_bytes);
         p->stage_out_bytes = out_bytes;
     }
     return ZLFFT_OK;
@@ -1617,7 +1626,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
     (void)tables();
     if (cudaMalloc(&p->d_err, sizeof(int)) != cudaSuccess || cudaMemset(p->d_err, 0, sizeof(int)) != cudaSuccess) {
         release(p);
-        return fail(ZLFFT_ERR_ALLOC, "error-word allocation failed");
+        return alloc_fail("error-word", sizeof(int));
     }
 
     const long long m = 1LL << cfft_order;
@@ -1626,7 +1635,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
     e = cudaMalloc(&p->d_tw, (p->tw_count + 1) * cx_bytes);
     if (e != cudaSuccess) {
         release(p);
-        return fail(ZLFFT_ERR_ALLOC, "twiddle allocation failed");
+        return alloc_fail("twiddle", (p->tw_count + 1) * cx_bytes);
     }
     if (p->tw_count > 0) {
         const unsigned blocks = (unsigned)((p->tw_count + 255) / 256);
@@ -1643,7 +1652,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
         const long long cnt = m >= 4 * l0 ? m - l0 : 0;
         if (cudaMalloc(&p->d_tws, (size_t)(cnt + 1) * cx_bytes) != cudaSuccess) {
             release(p);
-            return fail(ZLFFT_ERR_ALLOC, "twiddle allocation failed");
+            return alloc_fail("stage twiddle", (size_t)(cnt + 1) * cx_bytes);
         }
         if (cnt > 0) {
             const unsigned blocks = (unsigned)((cnt + 255) / 256);
@@ -1659,7 +1668,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
         const long long cnt = m / 2 + 1;
         if (cudaMalloc(&p->d_rw, cnt * cx_bytes) != cudaSuccess) {
             release(p);
-            return fail(ZLFFT_ERR_ALLOC, "RFFT twiddle allocation failed");
+            return alloc_fail("RFFT twiddle", cnt * cx_bytes);
         }
         const unsigned blocks = (unsigned)((cnt + 255) / 256);
         if (precision == ZLFFT_F32)
@@ -1680,7 +1689,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
         if (total) {
             if (cudaMalloc(&p->d_tctw, total * cx_bytes) != cudaSuccess) {
                 release(p);
-                return fail(ZLFFT_ERR_ALLOC, "tensor-core twiddle allocation failed");
+                return alloc_fail("tensor-core twiddle", total * cx_bytes);
             }
             for (int pi = 0; pi < zlfft::kMaxPasses; ++pi) {
                 const int l_in = tt.l_in[cfft_order - zlfft::kPassMinP][pi];
