@@ -4,10 +4,15 @@ Three independent CPU references for the reference's CFFT/RFFT path:
 
 * ``port``: the project's scalar C restatement of the reference algorithm
   (oracle/zlfft_oracle.c -> oracle/_build/libzloracle.so). Bit-identical to
-  the reference's micro-only Stockham path when twiddle tables agree.
+  the reference's micro-only Stockham path when twiddle tables agree, and,
+  inside ``hybrid()``, to its macro DIF path.
 * ``ref``: the reference's own headers, unchanged, compiled against the
   project's Highway-API shim (oracle/ref_capi.cpp -> oracle/_ref/libzlref.so).
   Present only where it was built (the build reads the reference sources).
+  A second build (oracle/_ref/libzlref_macro.so) links the same code with a
+  sysconf() stand-in reporting a small-cache host (oracle/ref_sysconf_wrap.cpp),
+  so that the reference's own switch sends orders >= 14 (float) / 13 (double)
+  down its Cooley-Tukey DIF macro path (src/common/zldsp_fft_common_execute.hpp:174-272).
 * ``fp64``: numpy.fft in complex128, scaled to the reference's unnormalised
   conventions: CFFT backward = N * ifft, RFFT backward = (N/2) * irfft
   (src/common/zldsp_fft_common_structure.hpp:47-135,
@@ -26,6 +31,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "libzloracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libzlref.so")
+REF_MACRO_SO = os.path.join(HERE, "_ref", "libzlref_macro.so")
+# (max_l1_order, switch_order) of the small-cache host that libzlref_macro.so
+# reports (oracle/ref_sysconf_wrap.cpp), per precision
+MACRO_HOST = {"f32": (10, 14), "f64": (9, 13)}
 
 AOS, SOA = 0, 1
 _c = ctypes
@@ -33,7 +42,7 @@ _sz = ctypes.c_size_t
 _vp = ctypes.c_void_p
 
 _port = None
-_ref = None
+_ref = {}
 
 
 def _dtypes(prec):
@@ -56,21 +65,25 @@ def port_lib():
                 _sz, _c.c_int, _c.c_int, fp, fp, _c.c_int, fp, fp, _sz, _c.c_int]
             getattr(lib, f"zlo_rfft_forward_{suf}").argtypes = [_sz, fp, _c.c_int, fp, fp, _sz]
             getattr(lib, f"zlo_rfft_backward_{suf}").argtypes = [_sz, fp, fp, _sz, fp]
+            getattr(lib, f"zlo_set_hybrid_{suf}").argtypes = [_c.c_int, _c.c_int]
+            getattr(lib, f"zlo_micro_order_{suf}").argtypes = [_sz]
+            getattr(lib, f"zlo_micro_order_{suf}").restype = _c.c_int
         _port = lib
     return _port
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_SO)
+def ref_available(macro: bool = False) -> bool:
+    return os.path.exists(REF_MACRO_SO if macro else REF_SO)
 
 
-def ref_lib():
-    """The reference's own code compiled against the Highway-API shim."""
-    global _ref
-    if _ref is None:
-        if not ref_available():
-            raise RuntimeError(f"reference build absent: {REF_SO} (run make -C oracle ref)")
-        lib = ctypes.CDLL(REF_SO)
+def ref_lib(macro: bool = False):
+    """The reference's own code compiled against the Highway-API shim; with
+    macro, the build whose cache probe reports a small-cache host."""
+    if macro not in _ref:
+        path = REF_MACRO_SO if macro else REF_SO
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference build absent: {path} (run make -C oracle ref)")
+        lib = ctypes.CDLL(path)
         lib.zlref_plan_create.restype = _vp
         lib.zlref_plan_create.argtypes = [_c.c_int, _c.c_int, _sz, _sz]
         lib.zlref_plan_destroy.argtypes = [_c.c_int, _vp]
@@ -78,8 +91,8 @@ def ref_lib():
         lib.zlref_rfft_exec.argtypes = [_c.c_int, _vp, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _sz]
         lib.zlref_switch_order.argtypes = [_c.c_int, _c.POINTER(_sz), _c.POINTER(_sz)]
         lib.zlref_cfft_roundtrip_repeat.argtypes = [_c.c_int, _vp, _vp, _vp, _vp, _sz]
-        _ref = lib
-    return _ref
+        _ref[macro] = lib
+    return _ref[macro]
 
 
 def _ptr(a, f):
@@ -87,6 +100,35 @@ def _ptr(a, f):
 
 
 # ----------------------------------------------------------------- port (C)
+class hybrid:
+    """Context manager: the port follows the reference's algorithm switch with
+    the given (max_l1_order, switch_order) (src/common/zldsp_fft_common_init.hpp:305-339):
+    CFFTs of order >= switch_order, and RFFTs whose inner CFFT is that large,
+    take the macro DIF path. Outside it the port is micro-only. Not thread-safe:
+    the setting is process-wide for the precision."""
+
+    def __init__(self, prec: str, max_l1_order: int, switch_order: int):
+        self.prec, self.l1, self.sw = prec, max_l1_order, switch_order
+
+    def __enter__(self):
+        getattr(port_lib(), f"zlo_set_hybrid_{self.prec}")(self.l1, self.sw)
+        return self
+
+    def __exit__(self, *exc):
+        getattr(port_lib(), f"zlo_set_hybrid_{self.prec}")(0, 1 << 30)
+        return False
+
+
+def macro_host(prec: str = "f32") -> hybrid:
+    """hybrid() with the small-cache host that libzlref_macro.so reports."""
+    return hybrid(prec, *MACRO_HOST[prec])
+
+
+def micro_order(order: int, prec: str = "f32") -> int:
+    """Micro order of the port's current switch for a CFFT of `order` (-1: micro-only)."""
+    return getattr(port_lib(), f"zlo_micro_order_{prec}")(order)
+
+
 def twiddles(order: int, prec: str = "f32") -> np.ndarray:
     """Unified twiddle table T[t] = exp(-2 pi i t / N), t < 3N/4, as the reference rounds it."""
     ft, ct = _dtypes(prec)
@@ -218,8 +260,8 @@ def istft_fp64(X: np.ndarray, hop: int, filt=None, win=None) -> np.ndarray:
 class RefPlan:
     """One reference CFFT/RFFT instance per thread (the reference is single-threaded)."""
 
-    def __init__(self, kind: str, order: int, prec: str = "f32", threads: int = 1):
-        self.lib = ref_lib()
+    def __init__(self, kind: str, order: int, prec: str = "f32", threads: int = 1, macro: bool = False):
+        self.lib = ref_lib(macro)
         self.prec = 0 if prec == "f32" else 1
         self.kind = kind
         self.order = order
@@ -299,10 +341,11 @@ class RefPlan:
         return out
 
 
-def ref_switch_order(prec: str = "f32"):
-    """(max_l1_order, switch_order) the reference derives from this host's caches."""
+def ref_switch_order(prec: str = "f32", macro: bool = False):
+    """(max_l1_order, switch_order) the reference derives from this host's caches
+    (with macro: from the small-cache host of libzlref_macro.so)."""
     a, b = _sz(), _sz()
-    ref_lib().zlref_switch_order(0 if prec == "f32" else 1, ctypes.byref(a), ctypes.byref(b))
+    ref_lib(macro).zlref_switch_order(0 if prec == "f32" else 1, ctypes.byref(a), ctypes.byref(b))
     return a.value, b.value
 
 

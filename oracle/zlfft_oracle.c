@@ -1,8 +1,10 @@
 /* TEST INFRASTRUCTURE ONLY — the oracle's scalar C restatement of the
- * reference's CFFT/RFFT algorithm (zldsp::fft, micro-only Stockham path:
+ * reference's CFFT/RFFT algorithm (zldsp::fft: the micro-only Stockham path,
  * src/common/zldsp_fft_common_execute.hpp:26-144 with the passes of
  * src/common/zldsp_fft_common_radix.hpp and the RFFT pre/post steps of
- * execute.hpp:318-536). Each function cites the reference lines it follows.
+ * execute.hpp:318-536; and, when zlo_set_hybrid_* selects it, the macro path
+ * of execute.hpp:174-272 with the DIF stages of radix.hpp:670-843). Each
+ * function cites the reference lines it follows.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
  * load this library, and only to check results or as the timed CPU baseline. The
@@ -12,8 +14,10 @@
  * is an fma() here, every other operation is a separate IEEE operation, and
  * the file is compiled with -ffp-contract=off (oracle/Makefile). With
  * identical twiddle tables the output is bit-identical to the reference's
- * micro-only path (checked in tests/test_oracle.py against the reference
- * headers compiled here through the Highway-API shim).
+ * micro-only path, and to its macro path under the same switch (checked in
+ * tests/test_oracle.py against the reference headers compiled here through
+ * the Highway-API shim, the macro path through a build whose cache probe
+ * reports a small-cache host).
  *
  * Pinning: the reference ships no tests or golden vectors for this path (its
  * CI accuracy scripts live in another repository), so this restatement is

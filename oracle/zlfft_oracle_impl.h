@@ -134,8 +134,15 @@ static void ZLO_SUF(pass_r4)(size_t n, size_t L, const CPX* x, CPX* y, const CPX
  * radix-8 first pass for odd orders >= 3, radix-4 first pass for even orders
  * >= 2, then radix-4 passes L = 4 or 8, x4 each, up to N
  * (src/common/zldsp_fft_common_init.hpp:193-206, execute.hpp:26-144,
- * kernel.hpp:19-144). x is clobbered. */
+ * kernel.hpp:19-144). x is clobbered. tw is the unified table of a length
+ * 2^tshift times N; entry t << tshift of it equals entry t of this order's own
+ * table bit for bit (the same double argument a = -2t/N, the exact power-of-two
+ * scaling cancels). */
+static void ZLO_SUF(dft_forward_t)(size_t order, CPX* x, CPX* y, const CPX* tw, unsigned tshift);
 static void ZLO_SUF(dft_forward)(size_t order, CPX* x, CPX* y, const CPX* tw) {
+    ZLO_SUF(dft_forward_t)(order, x, y, tw, 0);
+}
+static void ZLO_SUF(dft_forward_t)(size_t order, CPX* x, CPX* y, const CPX* tw, unsigned tshift) {
     const size_t n = (size_t)1 << order;
     if (order == 0) {
         y[0] = x[0];
@@ -159,7 +166,7 @@ static void ZLO_SUF(dft_forward)(size_t order, CPX* x, CPX* y, const CPX* tw) {
     unsigned s = 0;
     while ((n >> s) > 4 * L) ++s; /* n / (4L) = 1 << s */
     while (L < n) {
-        ZLO_SUF(pass_r4)(n, L, cur, nxt, tw, s);
+        ZLO_SUF(pass_r4)(n, L, cur, nxt, tw, s + tshift);
         CPX* t = cur;
         cur = nxt;
         nxt = t;
@@ -169,17 +176,106 @@ static void ZLO_SUF(dft_forward)(size_t order, CPX* x, CPX* y, const CPX* tw) {
     if (cur != y) memcpy(y, cur, n * sizeof(CPX));
 }
 
+/* ---------------------------------------------------------------- macro path
+ * The reference's algorithm switch (src/common/zldsp_fft_common_init.hpp:305-339):
+ * a CFFT of order >= switch_order runs as Cooley-Tukey DIF macro stages, then
+ * a micro Stockham FFT per segment, then a digit-reversed transposed store.
+ * The micro order is max_l1_order, or max_l1_order - 1 when order - max_l1_order
+ * is odd, so the macro stages are radix-4. The values come from the host's
+ * cache sizes in the reference (src/common/zldsp_fft_common_system.hpp:132-157);
+ * here the caller sets them. Default: never (micro-only), the reference's
+ * choice on a host whose caches put switch_order above every order used. */
+static int ZLO_SUF(g_max_l1) = 0;
+static int ZLO_SUF(g_switch) = 1 << 30;
+
+void ZLO_SUF(zlo_set_hybrid)(int max_l1_order, int switch_order) {
+    ZLO_SUF(g_max_l1) = max_l1_order;
+    ZLO_SUF(g_switch) = switch_order;
+}
+
+/* Micro order of the macro path for `order`, or -1 for the micro-only path. */
+int ZLO_SUF(zlo_micro_order)(size_t order) {
+    if ((long)order < (long)ZLO_SUF(g_switch)) return -1;
+    const int l1 = ZLO_SUF(g_max_l1);
+    return ((long)order - l1) % 2 != 0 ? l1 - 1 : l1;
+}
+
+/* One radix-4 DIF stage in place, butterfly stride w: for each block of 4w
+ * points and j < w, x[j + q*w] (q = 0..3) -> DFT4 with the twiddle W_{4w}^{m j}
+ * applied to output m AFTER the butterfly; outputs stay at their positions
+ * (src/common/zldsp_fft_common_radix.hpp:670-751 first stage with the loads,
+ * :762-843 the in-place stages). The twiddle of the reference's stage table
+ * (init.hpp:227-274: cospi(m * j * (-2/(4w)))) is entry (m*j) << s of the
+ * unified table, n/(4w) = 1 << s. */
+static void ZLO_SUF(dif_stage)(size_t n, size_t w, CPX* x, const CPX* tw, unsigned s) {
+    for (size_t blk = 0; blk < n; blk += 4 * w) {
+        CPX* p = x + blk;
+        for (size_t j = 0; j < w; ++j) {
+            const CPX a = p[j], b = p[j + w], c = p[j + 2 * w], d = p[j + 3 * w];
+            const CPX t0 = {a.r + c.r, a.i + c.i}, t1 = {a.r - c.r, a.i - c.i};
+            const CPX t2 = {b.r + d.r, b.i + d.i}, t3 = {b.r - d.r, b.i - d.i};
+            const CPX y0 = {t0.r + t2.r, t0.i + t2.i};
+            const CPX y2 = {t0.r - t2.r, t0.i - t2.i};
+            const CPX y1 = {t1.r + t3.i, t1.i - t3.r};
+            const CPX y3 = {t1.r - t3.i, t1.i + t3.r};
+            p[j] = y0;
+            p[j + w] = ZLO_SUF(cmul)(y1, tw[(1 * j) << s]);
+            p[j + 2 * w] = ZLO_SUF(cmul)(y2, tw[(2 * j) << s]);
+            p[j + 3 * w] = ZLO_SUF(cmul)(y3, tw[(3 * j) << s]);
+        }
+    }
+}
+
+/* Base-4 digit reversal of c over nd digits (init.hpp:282-296). */
+static size_t ZLO_SUF(digit_rev4)(size_t c, size_t nd) {
+    size_t r = 0;
+    for (size_t d = 0; d < nd; ++d) {
+        r = (r << 2) | (c & 3);
+        c >>= 2;
+    }
+    return r;
+}
+
+/* Forward macro-path DFT of a (length 1<<order, already direction-swapped),
+ * clobbering a; output element k*S + c (S = segments) goes to (re, im, step)
+ * through the store swap (src/common/zldsp_fft_common_execute.hpp:174-272):
+ * column c is the micro FFT of the segment at digit_rev4(c). b is scratch of
+ * at least 2 * 2^micro points. */
+static void ZLO_SUF(macro_forward)(size_t order, int micro, int forward, const CPX* tw, CPX* a, CPX* b,
+                                   ZLO_F* out_re, ZLO_F* out_im, size_t out_step) {
+    const size_t n = (size_t)1 << order;
+    const size_t nm = (order - (size_t)micro) / 2;
+    for (size_t i = 0; i < nm; ++i) ZLO_SUF(dif_stage)(n, n >> (2 * i + 2), a, tw, (unsigned)(2 * i));
+    const size_t m = (size_t)1 << micro, segs = n >> micro;
+    for (size_t c = 0; c < segs; ++c) {
+        memcpy(b, a + ZLO_SUF(digit_rev4)(c, nm) * m, m * sizeof(CPX));
+        ZLO_SUF(dft_forward_t)((size_t)micro, b, b + m, tw, (unsigned)(order - (size_t)micro));
+        const CPX* y = b + m;
+        for (size_t k = 0; k < m; ++k) {
+            const size_t o = (k * segs + c) * out_step;
+            out_re[o] = forward ? y[k].r : y[k].i;
+            out_im[o] = forward ? y[k].i : y[k].r;
+        }
+    }
+}
+
 /* Complex FFT of one transform with the reference's conventions:
  * forward = DFT with exp(-i...), backward = swap(DFT(swap(x))) = unnormalised
  * inverse (src/common/zldsp_fft_common_structure.hpp:47-135).
  * Layout is given by (re, im, step): AoS is (p, p+1, 2), SoA is (r, i, 1).
- * tw is the table of zlo_twiddles(order); a and b are scratch of N points. */
+ * tw is the table of zlo_twiddles(order); a and b are scratch of N points.
+ * Orders at or above the switch take the macro path (zlo_set_hybrid). */
 static void ZLO_SUF(cfft_core)(size_t order, int forward, const CPX* tw, const ZLO_F* in_re, const ZLO_F* in_im,
                                size_t in_step, ZLO_F* out_re, ZLO_F* out_im, size_t out_step, CPX* a, CPX* b) {
     const size_t n = (size_t)1 << order;
     for (size_t k = 0; k < n; ++k) {
         const ZLO_F r = in_re[k * in_step], i = in_im[k * in_step];
         a[k] = forward ? (CPX){r, i} : (CPX){i, r};
+    }
+    const int micro = ZLO_SUF(zlo_micro_order)(order);
+    if (micro >= 0 && (size_t)micro + 2 <= order) {
+        ZLO_SUF(macro_forward)(order, micro, forward, tw, a, b, out_re, out_im, out_step);
+        return;
     }
     ZLO_SUF(dft_forward)(order, a, b, tw);
     for (size_t k = 0; k < n; ++k) {

@@ -10,7 +10,18 @@ kernels where the reference sources are not present.
 
 Inputs: complex re, im ~ U[-1, 1) and real frames ~ U[-1, 1), numpy PCG64
 seeds 7000 + order. Outputs are exactly what the reference writes.
+
+reference_macro_{f32,f64}.npz come from the same reference code linked with a
+sysconf() stand-in that reports a small-cache host
+(oracle/_ref/libzlref_macro.so), so that the reference takes its Cooley-Tukey
+DIF macro path from CFFT order 14 (float) / 13 (double). They hold the full
+vectors of the smallest macro order, and for every macro order up to 22 / 21
+(CFFT forward and backward; RFFT forward, forward_sqr_mag and backward of the
+RFFT whose inner CFFT has that order) the SHA-256 of the reference's output
+bytes on inputs regenerated from the seeds 9000 + order (complex) and
+9500 + order (real): one transform each, too large to store in full.
 """
+import hashlib
 import os
 import sys
 
@@ -24,6 +35,47 @@ from oracle import oracle as O  # noqa: E402
 CFFT_ORDERS = list(range(0, 11))
 RFFT_ORDERS = list(range(1, 12))
 BATCH = 2
+
+
+MACRO_ORDERS = {"f32": list(range(14, 23)), "f64": list(range(13, 22))}
+
+
+def macro_inputs(prec, order):
+    """Seeded inputs of the macro fixtures for CFFT order `order`: a complex
+    transform, a real frame of twice its length and a bin vector for the RFFT."""
+    ft, ct = (np.float32, np.complex64) if prec == "f32" else (np.float64, np.complex128)
+    n = 1 << order
+    rng = np.random.default_rng(9000 + order)
+    x = (rng.uniform(-1, 1, (1, n)) + 1j * rng.uniform(-1, 1, (1, n))).astype(ct)
+    rng = np.random.default_rng(9500 + order)
+    xr = rng.uniform(-1, 1, (1, 2 * n)).astype(ft)
+    X = (rng.uniform(-1, 1, (1, n + 1)) + 1j * rng.uniform(-1, 1, (1, n + 1))).astype(ct)
+    return x, xr, X
+
+
+def sha(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def macro_main():
+    for prec in ("f32", "f64"):
+        data = {}
+        for i, order in enumerate(MACRO_ORDERS[prec]):
+            x, xr, X = macro_inputs(prec, order)
+            plan = O.RefPlan("c2c", order, prec, macro=True)
+            fwd, bwd = plan.cfft(x, True), plan.cfft(x, False)
+            plan.close()
+            rp = O.RefPlan("r2c", order + 1, prec, macro=True)
+            rf, rs, rb = rp.rfft_forward(xr), rp.rfft_forward(xr, sqr_mag=True), rp.rfft_backward(X)
+            rp.close()
+            if i == 0:
+                data[f"c2c_{order}_in"] = x
+                data[f"c2c_{order}_fwd"] = fwd
+                data[f"c2c_{order}_bwd"] = bwd
+            data[f"sha_{order}"] = np.array([sha(fwd), sha(bwd), sha(rf), sha(rs), sha(rb)])
+        path = os.path.join(HERE, f"reference_macro_{prec}.npz")
+        np.savez_compressed(path, **data)
+        print(path, os.path.getsize(path), "bytes")
 
 
 def main():
@@ -57,3 +109,4 @@ def main():
 
 if __name__ == "__main__":
     main()
+    macro_main()

@@ -188,3 +188,102 @@ def test_istft_slicing_recipe_on_the_oracle(oracle):
                 a, b = f0 * hop, (total if f1 == nf else f1 * hop)
                 out[a:b] = part[a - g0 * hop:b - g0 * hop]
             assert np.array_equal(out, whole), (hop, cuts)
+
+
+# ---------------------------------------------------------------- the reference's macro DIF path
+# On a host with small caches the reference runs CFFTs of order >= switch_order
+# as Cooley-Tukey DIF macro stages + per-segment Stockham + a digit-reversed
+# transposed store (src/common/zldsp_fft_common_execute.hpp:174-272). The
+# restatement follows it inside oracle.hybrid(); these tests pin it.
+
+def _macro_golden(prec):
+    return np.load(os.path.join(GOLDEN, f"reference_macro_{prec}.npz"))
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_port_macro_matches_reference_golden(oracle, prec):
+    """Full vectors at the smallest macro order, and SHA-256 of the reference's
+    outputs for every macro order up to 22 (float) / 21 (double), made by
+    tests/golden/make_golden.py from the macro-path build of the reference."""
+    import hashlib
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    g = _macro_golden(prec)
+    orders = mg.MACRO_ORDERS[prec]
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()  # noqa: E731
+    with oracle.macro_host(prec):
+        o0 = orders[0]
+        x = g[f"c2c_{o0}_in"]
+        assert np.array_equal(oracle.cfft_port(x, True), g[f"c2c_{o0}_fwd"])
+        assert np.array_equal(oracle.cfft_port(x, False), g[f"c2c_{o0}_bwd"])
+        for order in orders:
+            assert oracle.micro_order(order, prec) > 0, order
+            x, xr, X = mg.macro_inputs(prec, order)
+            got = [sha(oracle.cfft_port(x, True)), sha(oracle.cfft_port(x, False)), sha(oracle.rfft_forward_port(xr)),
+                   sha(oracle.rfft_forward_port(xr, sqr_mag=True)), sha(oracle.rfft_backward_port(X))]
+            assert got == list(g[f"sha_{order}"]), order
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
+                                                    "libzlref_macro.so")), reason="macro-path reference build absent")
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+def test_port_macro_bitwise_equals_reference_macro_library(oracle, prec, ft, ct):
+    """The restatement's macro path equals the reference's, bit for bit, in every
+    layout pairing: CFFT orders from the switch to 19 (both micro-order
+    parities), RFFT forward / forward_sqr_mag / backward in AoS and SoA."""
+    l1, switch = oracle.ref_switch_order(prec, macro=True)
+    assert (l1, switch) == oracle.MACRO_HOST[prec]
+    rng = np.random.default_rng(1234)
+    with oracle.macro_host(prec):
+        for order in range(switch - 1, 20):
+            n = 1 << order
+            b = 2 if order < 17 else 1
+            x = (rng.uniform(-1, 1, (b, n)) + 1j * rng.uniform(-1, 1, (b, n))).astype(ct)
+            plan = oracle.RefPlan("c2c", order, prec, macro=True)
+            for fwd in (True, False):
+                assert np.array_equal(oracle.cfft_port(x, fwd), plan.cfft(x, fwd)), (order, fwd)
+            re, im = np.ascontiguousarray(x.real), np.ascontiguousarray(x.imag)
+            for fwd in (True, False):
+                ref_aos = plan.cfft(x, fwd)
+                for il, inp in ((oracle.AOS, x), (oracle.SOA, (re, im))):
+                    for ol in (oracle.AOS, oracle.SOA):
+                        y = plan.cfft(inp, fwd, il, ol)
+                        y = y if ol == oracle.AOS else (y[0] + 1j * y[1]).astype(ct)
+                        assert np.array_equal(y, ref_aos), (order, fwd, il, ol)
+            plan.close()
+            xr = rng.uniform(-1, 1, (b, 2 * n)).astype(ft)
+            rp = oracle.RefPlan("r2c", order + 1, prec, macro=True)
+            X = rp.rfft_forward(xr)
+            assert np.array_equal(oracle.rfft_forward_port(xr), X), order
+            s0, s1 = rp.rfft_forward(xr, layout=oracle.SOA)
+            assert np.array_equal((s0 + 1j * s1).astype(ct), X), order
+            assert np.array_equal(oracle.rfft_forward_port(xr, True), rp.rfft_forward(xr, sqr_mag=True)), order
+            assert np.array_equal(oracle.rfft_backward_port(X), rp.rfft_backward(X)), order
+            Xs = (np.ascontiguousarray(X.real), np.ascontiguousarray(X.imag))
+            assert np.array_equal(oracle.rfft_backward_port(X), rp.rfft_backward(Xs, layout=oracle.SOA)), order
+            rp.close()
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+def test_port_macro_within_fp64_tolerance(oracle, prec, ft, ct):
+    """The macro path is as accurate as the micro-only one, and a different
+    rounding of the same transform (the two differ in their bits)."""
+    rng = np.random.default_rng(77)
+    l1, switch = oracle.MACRO_HOST[prec]
+    for order in range(switch, switch + 5):
+        n = 1 << order
+        x = (rng.uniform(-1, 1, (1, n)) + 1j * rng.uniform(-1, 1, (1, n))).astype(ct)
+        micro_only = oracle.cfft_port(x, True)
+        with oracle.hybrid(prec, l1, switch):
+            ym = oracle.cfft_port(x, True)
+            yb = oracle.cfft_port(x, False)
+            xr = rng.uniform(-1, 1, (1, 2 * n)).astype(ft)
+            X = oracle.rfft_forward_port(xr)
+        tol = oracle.tolerance(order, prec)
+        assert oracle.rel_l2(ym, oracle.cfft_fp64(x, True)).max() <= tol
+        assert oracle.rel_l2(yb, oracle.cfft_fp64(x, False)).max() <= tol
+        assert oracle.rel_l2(X, oracle.rfft_fp64(xr)).max() <= oracle.tolerance(order + 1, prec)
+        assert not np.array_equal(ym, micro_only)
+    assert oracle.micro_order(switch, prec) == -1  # outside hybrid(): micro-only again
