@@ -24,10 +24,13 @@ constexpr int precision() {
 }
 
 // Move-only owner of one zlfft plan (the reference objects are move-only too:
-// they own hwy::AlignedFreeUniquePtr buffers).
+// they own hwy::AlignedFreeUniquePtr buffers). Like the reference's
+// constructors, the plan picks its algorithm from this host's cache sizes
+// (ZLFFT_MODE_HOST: src/common/zldsp_fft_common_init.hpp:305-339), so the
+// results are the ones the reference gives on this host.
 class Plan {
 public:
-    Plan(int kind, int precision, size_t order) { check(zlfft_plan_create(&h_, kind, precision, order, ZLFFT_MODE_PLAIN, -1)); }
+    Plan(int kind, int precision, size_t order) { check(zlfft_plan_create(&h_, kind, precision, order, ZLFFT_MODE_HOST, -1)); }
     ~Plan() { zlfft_plan_destroy(h_); }
     Plan(const Plan&) = delete;
     Plan& operator=(const Plan&) = delete;

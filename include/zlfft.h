@@ -68,6 +68,9 @@ typedef struct zlfft_plan_s* zlfft_plan;
 #define ZLFFT_MODE_FAST 5    /* plain CUDA-core form whose multi-pass radix-16 groups build their
                                 twiddles from two table values (fewer loads): within the FP bar,
                                 not bit-identical to the reference; single-tile sizes as PLAIN */
+#define ZLFFT_MODE_HOST 6    /* PLAIN, following the reference's own algorithm switch as the caches of
+                                THIS host set it (see zlfft_host_switch_order): bit-identical (FP32)
+                                to the reference's output on this host, macro path included */
 
 /* Create a plan for one transform size.
  * Replaces the constructors CFFT<F>::CFFT(size_t order)
@@ -77,6 +80,36 @@ typedef struct zlfft_plan_s* zlfft_plan;
  * above). Twiddle tables are generated on the device in FP64 and rounded to
  * the plan's precision. device < 0 means the current device. */
 ZLFFT_API int zlfft_plan_create(zlfft_plan* plan, int kind, int precision, size_t order, int mode, int device);
+
+/* As zlfft_plan_create with mode ZLFFT_MODE_PLAIN, following the reference's
+ * algorithm switch with the given values instead of the arithmetic of one
+ * path for every order (src/common/zldsp_fft_common_init.hpp:305-339, the
+ * constructors' init_cfft_state): a CFFT whose order is >= switch_order (for
+ * an RFFT, its inner CFFT of order - 1) runs the reference's macro path -
+ * radix-4 Cooley-Tukey DIF stages (src/common/zldsp_fft_common_radix.hpp:670-843),
+ * then a Stockham FFT of the micro order per segment and a digit-reversed
+ * transposed store (src/common/zldsp_fft_common_execute.hpp:174-272) - with
+ * micro order max_l1_order, or max_l1_order - 1 when order - max_l1_order is
+ * odd. Below switch_order the plan is the plain micro-only plan. With the
+ * (max_l1_order, switch_order) that get_switch_order<F>()
+ * (src/common/zldsp_fft_common_system.hpp:132-157) returns on some host, the
+ * FP32 output is bit-identical to the reference's on that host (FP64: within
+ * the FP64 bar). Micro orders 8-12 are built (ZLFFT_ERR_UNSUPPORTED
+ * otherwise). Macro-path plans run through zlfft_exec_host*, zlfft_exec_device
+ * and zlfft_exec_device_noalloc; the STFT entry points refuse them. */
+ZLFFT_API int zlfft_plan_create_hybrid(zlfft_plan* plan, int kind, int precision, size_t order, int max_l1_order,
+                                       int switch_order, int device);
+
+/* The (max_l1_order, switch_order) the reference computes on this host for
+ * precision F (get_switch_order<F>, src/common/zldsp_fft_common_system.hpp:132-157):
+ * the same cache-size queries (sysconf on Linux, the reference's defaults
+ * where a query gives nothing) and arithmetic. ZLFFT_MODE_HOST plans use them. */
+ZLFFT_API int zlfft_host_switch_order(int precision, size_t* max_l1_order, size_t* switch_order);
+
+/* The micro order of a plan on the macro path, or -1 when it runs the
+ * micro-only path. No reference counterpart (CFFTState::micro_cfft_order,
+ * src/common/zldsp_fft_common_init.hpp:25-43, is internal there). */
+ZLFFT_API int zlfft_plan_get_micro_order(zlfft_plan plan, int* micro_order);
 
 /* Release a plan and every buffer it owns. Replaces the reference objects'
  * destructors (members freed by hwy::AlignedFreeUniquePtr,

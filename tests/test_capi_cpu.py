@@ -154,3 +154,20 @@ def test_cpp_dropin_headers_compile_and_link(tmp_path):
     """The reference's README usage compiles unchanged against the drop-in
     headers (include/zldsp_fft_cuda/) and links against libzlfft_cuda.so."""
     _build_dropin(tmp_path)
+
+
+def test_host_switch_order_is_the_references():
+    """zlfft_host_switch_order restates the reference's get_switch_order<F>
+    (src/common/zldsp_fft_common_system.hpp:132-157) from the same cache
+    queries: on this host it gives the reference's own values."""
+    from oracle import oracle as O
+    for prec, dt in (("f32", 0), ("f64", 1)):
+        a, b = ctypes.c_size_t(), ctypes.c_size_t()
+        assert C.lib().zlfft_host_switch_order(dt, ctypes.byref(a), ctypes.byref(b)) == C.OK
+        if O.ref_available():
+            assert (a.value, b.value) == O.ref_switch_order(prec)
+        assert a.value >= 1 and b.value >= a.value + 4
+    assert C.lib().zlfft_host_switch_order(7, ctypes.byref(a), ctypes.byref(b)) == C.ERR_INVALID_ARG
+    assert C.lib().zlfft_plan_create_hybrid(None, 0, 0, 16, 10, 14, -1) == C.ERR_INVALID_ARG
+    h = ctypes.c_void_p()
+    assert C.lib().zlfft_plan_create_hybrid(ctypes.byref(h), 0, 0, 16, -3, 14, -1) == C.ERR_INVALID_ARG

@@ -9,13 +9,14 @@ Layers:
 """
 from . import _capi
 from ._capi import (AOS, BACKWARD, C2C, F32, F64, FORWARD, FORWARD_SQR_MAG, MODE_PLAIN, MODE_TC_BF16,
-                    MODE_FAST, MODE_TC_FP16, MODE_TC_TF32, MODE_TUNED, R2C, SCHED_GRAPH, SCHED_PER_ORDER, SCHED_PERSISTENT,
-                    SOA, ZlfftError)
-from .fft import CFFT, RFFT, MixedBatch, Plan, autotune, tuning, tuning_clear, tuning_load, tuning_save
+                    MODE_FAST, MODE_HOST, MODE_TC_FP16, MODE_TC_TF32, MODE_TUNED, R2C, SCHED_GRAPH, SCHED_PER_ORDER,
+                    SCHED_PERSISTENT, SOA, ZlfftError)
+from .fft import (CFFT, RFFT, MixedBatch, Plan, autotune, host_switch_order, tuning, tuning_clear, tuning_load,
+                  tuning_save)
 
 __all__ = [
     "CFFT", "RFFT", "Plan", "MixedBatch", "ZlfftError", "AOS", "SOA", "C2C", "R2C", "F32", "F64", "FORWARD", "BACKWARD",
     "FORWARD_SQR_MAG", "MODE_PLAIN", "MODE_TC_FP16", "MODE_TC_BF16", "MODE_TC_TF32", "MODE_TUNED", "MODE_FAST",
-    "SCHED_PER_ORDER", "SCHED_PERSISTENT", "SCHED_GRAPH", "autotune", "tuning", "tuning_save", "tuning_load",
-    "tuning_clear",
+    "MODE_HOST", "SCHED_PER_ORDER", "SCHED_PERSISTENT", "SCHED_GRAPH", "autotune", "host_switch_order", "tuning",
+    "tuning_save", "tuning_load", "tuning_clear",
 ]

@@ -26,7 +26,7 @@ C2C, R2C = 0, 1
 F32, F64 = 0, 1
 AOS, SOA = 0, 1
 FORWARD, BACKWARD, FORWARD_SQR_MAG = 0, 1, 2
-MODE_PLAIN, MODE_TC_FP16, MODE_TC_BF16, MODE_TC_TF32, MODE_TUNED, MODE_FAST = 0, 1, 2, 3, 4, 5
+MODE_PLAIN, MODE_TC_FP16, MODE_TC_BF16, MODE_TC_TF32, MODE_TUNED, MODE_FAST, MODE_HOST = 0, 1, 2, 3, 4, 5, 6
 SCHED_PER_ORDER, SCHED_PERSISTENT, SCHED_GRAPH = 0, 1, 2
 
 
@@ -46,6 +46,9 @@ class Tuning(ctypes.Structure):
 # every symbol include/zlfft.h declares
 EXPORTS = (
     "zlfft_plan_create",
+    "zlfft_plan_create_hybrid",
+    "zlfft_host_switch_order",
+    "zlfft_plan_get_micro_order",
     "zlfft_plan_destroy",
     "zlfft_plan_get_size",
     "zlfft_plan_get_order",
@@ -100,6 +103,9 @@ def lib() -> ctypes.CDLL:
         L = ctypes.CDLL(LIB_PATH)
         sz, vp, i = ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int
         L.zlfft_plan_create.argtypes = [ctypes.POINTER(vp), i, i, sz, i, i]
+        L.zlfft_plan_create_hybrid.argtypes = [ctypes.POINTER(vp), i, i, sz, i, i, i]
+        L.zlfft_host_switch_order.argtypes = [i, ctypes.POINTER(sz), ctypes.POINTER(sz)]
+        L.zlfft_plan_get_micro_order.argtypes = [vp, ctypes.POINTER(i)]
         L.zlfft_plan_destroy.argtypes = [vp]
         L.zlfft_plan_get_size.argtypes = [vp, ctypes.POINTER(sz)]
         L.zlfft_plan_get_order.argtypes = [vp, ctypes.POINTER(sz)]

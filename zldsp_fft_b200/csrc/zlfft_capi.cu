@@ -9,6 +9,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
@@ -21,6 +22,7 @@
 #include "../../include/zlfft.h"
 #include "zlfft_istft.cuh"
 #include "zlfft_launch.cuh"
+#include "zlfft_macro.cuh"
 #include "zlfft_mixed.cuh"
 
 namespace {
@@ -155,7 +157,13 @@ struct TablesHolder {
     zlfft::TcPassTable tc{};
     zlfft::IstftTable i32{};
     zlfft::IstftTable i64{};
+    zlfft::MacroTable m32{};
+    zlfft::MacroTable m64{};
     TablesHolder() {
+        zlfft::fill_macro_dif_f32(m32);
+        zlfft::fill_macro_seg_f32(m32);
+        zlfft::fill_macro_dif_f64(m64);
+        zlfft::fill_macro_seg_f64(m64);
         zlfft::fill_istft_f32(i32);
         zlfft::fill_istft_f64(i64);
         zlfft::fill_tc_pass_a(tc);
@@ -307,6 +315,13 @@ struct zlfft_plan_s {
     bool fast_form = false; // multi-pass radix-16 groups with fast twiddles (ZLFFT_MODE_FAST)
     bool fuse_split = false;  // RFFT forward: split fused into the last pass (else its own kernel)
     int store_tma = -1;       // first pass output by TMA tensor stores (-1: the precision's default)
+    // The reference's algorithm switch (src/common/zldsp_fft_common_init.hpp:305-339), where the plan
+    // follows one: a CFFT order >= switch_order runs the macro path (zlfft_macro.cuh) with this micro
+    // order; -1: the micro-only Stockham path
+    int micro = -1;
+    int max_l1 = -1, switch_order = -1;  // the switch the plan follows (-1: none)
+    void* d_mtw = nullptr;                // macro path: unified twiddle table of the micro order
+    void* d_mtws = nullptr;               // macro path: per-stage tables of the micro order
     std::mutex mu;            // the host path's staging buffers and streams
     std::mutex scratch_mu;    // first-use creation of the scratch, lanes and their events
 };
@@ -331,6 +346,8 @@ void release(zlfft_plan p) {
     if (p->d_tws) cudaFree(p->d_tws);
     if (p->d_rw) cudaFree(p->d_rw);
     if (p->d_tctw) cudaFree(p->d_tctw);
+    if (p->d_mtw) cudaFree(p->d_mtw);
+    if (p->d_mtws) cudaFree(p->d_mtws);
     if (p->d_err) cudaFree(p->d_err);
     if (p->d_scratch) cudaFree(p->d_scratch);
     for (int i = 0; i < 2; ++i) {
@@ -674,8 +691,12 @@ bool tile14(const zlfft_plan_s* p) {
     return p->cfft_order == 14 && p->prec == ZLFFT_F32 && !p->tc_form;
 }
 
-int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,
-                     void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, cudaStream_t stream) {
+// Argument checks shared by the device entry points (zlfft_exec_device and
+// zlfft_exec_device_noalloc), and the kernel arguments they lead to. *a is
+// filled only when the call has work (rc 0 and batch > 0).
+int prepare_device_call(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,
+                        void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride,
+                        zlfft::TileArgs* a) {
     int rc = validate_op(p, op, in_layout, out_layout);
     if (rc) return rc;
     const Extents ex = extents(p, op);
@@ -707,34 +728,200 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     if (rc) return rc;
     if (batch == 0) return ZLFFT_OK;
 
-    zlfft::TileArgs a{};
-    a.in0 = in0;
-    a.in1 = in_soa ? in1 : nullptr;
-    a.out0 = out0;
-    a.out1 = out_soa ? out1 : nullptr;
-    a.batch = (long long)batch;
+    *a = zlfft::TileArgs{};
+    a->in0 = in0;
+    a->in1 = in_soa ? in1 : nullptr;
+    a->out0 = out0;
+    a->out1 = out_soa ? out1 : nullptr;
+    a->batch = (long long)batch;
     // Strides in units of the element each kernel indexes: real sides of an
     // RFFT are indexed as complex pairs, except the squared-magnitude output.
-    a.in_stride = (long long)(ex.in_complex ? in_stride : in_stride / 2);
-    a.out_stride = (long long)((ex.out_complex || op == ZLFFT_FORWARD_SQR_MAG) ? out_stride : out_stride / 2);
-    a.tw = p->d_tw;
-    a.tws = p->d_tws;
-    a.rw = p->d_rw;
-    a.err = p->d_err;
+    a->in_stride = (long long)(ex.in_complex ? in_stride : in_stride / 2);
+    a->out_stride = (long long)((ex.out_complex || op == ZLFFT_FORWARD_SQR_MAG) ? out_stride : out_stride / 2);
+    a->tw = p->d_tw;
+    a->tws = p->d_tws;
+    a->rw = p->d_rw;
+    a->err = p->d_err;
     // Bulk (TMA) copies need 16-byte aligned sources: the bases and the
     // per-transform stride in bytes. The kernel reads directly otherwise.
     {
         const size_t in_elem_bytes = in_soa ? p->esize : 2 * p->esize;  // complex or pairs of reals
         const bool al = aligned(in0, 16) && (!in_soa || aligned(in1, 16)) &&
-                        (batch == 1 || ((size_t)a.in_stride * in_elem_bytes) % 16 == 0);
-        a.tma = (al && p->use_tma) ? 1 : 0;
+                        (batch == 1 || ((size_t)a->in_stride * in_elem_bytes) % 16 == 0);
+        a->tma = (al && p->use_tma) ? 1 : 0;
     }
-
-    const int dop = device_op_code(p, op);
     // backward RFFT tiles stage their bins by cp.async: element alignment suffices
-    if (dop == zlfft::kC2RBwd) a.tma = p->use_tma ? 1 : 0;
+    if (device_op_code(p, op) == zlfft::kC2RBwd) a->tma = p->use_tma ? 1 : 0;
+    return ZLFFT_OK;
+}
+
+// Intermediate buffers of one macro-path execution: chunks of `chunk`
+// transforms alternate between `lanes` pipelines; pipeline i owns buf[i][0]
+// and buf[i][1] (each `chunk` transforms long) and runs on stream[i] (lanes
+// == 1: the caller's stream).
+struct MacroScratch {
+    char* buf[2][2];
+    long long chunk;
+    int lanes;
+    cudaStream_t stream[2];
+};
+
+// The reference's macro path (zlfft_macro.cuh) over a batch: for each chunk,
+// [RFFT backward pre-step] -> DIF pass(es) -> segment FFTs with the
+// transposed store -> [RFFT forward split]. The DIF stages of one transform
+// run in one pass up to 5 stages (1024-point units), else in two passes.
+int exec_macro(zlfft_plan_s* p, int dop, int in_layout, int out_layout, const zlfft::TileArgs& a, cudaStream_t st,
+               const zlfft::LaunchCtx& ctx, const MacroScratch& sc) {
+    const int O = p->cfft_order, m = p->micro;
+    const int nm = (O - m) / 2;
+    const zlfft::MacroTable& t = p->prec == ZLFFT_F32 ? tables().m32 : tables().m64;
+    int gp[2] = {nm, 0};
+    int npass = 1;
+    if (nm > zlfft::kMacroMaxG) {
+        gp[0] = nm / 2;
+        gp[1] = nm - nm / 2;
+        npass = 2;
+    }
+    const size_t cx = 2 * p->esize;
+    const long long n = 1LL << O;
+    const bool fwd = (dop == zlfft::kC2CFwd || dop == zlfft::kR2CFwd || dop == zlfft::kR2CSqrMag);
+    const bool r2c = (dop == zlfft::kR2CFwd || dop == zlfft::kR2CSqrMag);
+    const bool c2r = (dop == zlfft::kC2RBwd);
+    const int il = r2c ? ZLFFT_AOS : in_layout;   // R2C: real input read as complex pairs
+    const int ol = c2r ? ZLFFT_AOS : out_layout;  // C2R: real output written as complex pairs
+    const size_t in_elem = (in_layout == ZLFFT_SOA && !r2c) ? p->esize : cx;
+    const size_t out_elem = (out_layout == ZLFFT_SOA && !c2r) ? p->esize : cx;
+    for (long long b0 = 0, ci = 0; b0 < a.batch; b0 += sc.chunk, ++ci) {
+        const long long nb = std::min<long long>(sc.chunk, a.batch - b0);
+        const int lane = (int)(ci % sc.lanes);
+        const cudaStream_t s = sc.lanes > 1 ? sc.stream[lane] : st;
+        char* const* buf = sc.buf[lane];
+        const char* ui0 = static_cast<const char*>(a.in0) + b0 * a.in_stride * in_elem;
+        const char* ui1 = a.in1 ? static_cast<const char*>(a.in1) + b0 * a.in_stride * in_elem : nullptr;
+        char* uo0 = static_cast<char*>(a.out0) + b0 * a.out_stride * (dop == zlfft::kR2CSqrMag ? p->esize : out_elem);
+        char* uo1 = a.out1 ? static_cast<char*>(a.out1) + b0 * a.out_stride * out_elem : nullptr;
+        cudaError_t e;
+        const void* src0 = ui0;
+        const void* src1 = ui1;
+        long long src_stride = a.in_stride;
+        int src_layout = il;
+        int next = 0;  // the scratch buffer the next kernel writes
+        if (c2r) {
+            e = p->prec == ZLFFT_F32 ? launch_pre<float>(p, in_layout, ui0, ui1, buf[0], nb, a.in_stride, s, ctx)
+                                     : launch_pre<double>(p, in_layout, ui0, ui1, buf[0], nb, a.in_stride, s, ctx);
+            if (e != cudaSuccess) return cuda_fail(e, "rfft pre-step launch");
+            src0 = buf[0];
+            src1 = nullptr;
+            src_stride = n;
+            src_layout = ZLFFT_AOS;
+            next = 1;
+        }
+        int i0 = 0;
+        for (int pi = 0; pi < npass; ++pi) {
+            const int G = gp[pi];
+            const bool last = (pi + 1 == npass);
+            zlfft::DifArgs da{};
+            da.in0 = src0;
+            da.in1 = src1;
+            da.out = buf[next];
+            da.batch = nb;
+            da.in_stride = src_stride;
+            da.out_stride = n;
+            da.tws = p->d_tws;
+            da.order = O;
+            da.i0 = i0;
+            da.wlog = O - 2 * (i0 + G);
+            da.nm = nm;
+            da.mlog = m;
+            const zlfft::DifLaunchFn fn =
+                pi == 0 ? t.first[G - 1][fwd ? 1 : 0][src_layout][last ? 1 : 0] : t.mid[G - 1][last ? 1 : 0];
+            e = fn(da, s, ctx);
+            if (e != cudaSuccess) return cuda_fail(e, "DIF pass launch");
+            src0 = buf[next];
+            src1 = nullptr;
+            src_stride = n;
+            next ^= 1;
+            i0 += G;
+        }
+        // segment FFTs + transposed store: to the output, or (RFFT forward) to scratch for the split
+        zlfft::SegArgs sa{};
+        sa.t.in0 = src0;
+        sa.t.batch = nb << (2 * nm);
+        sa.t.in_stride = 1LL << m;
+        sa.t.out_stride = 1LL << m;
+        sa.t.tw = p->d_mtw;
+        sa.t.tws = p->d_mtws;
+        sa.t.err = p->d_err;
+        sa.t.tma = p->use_tma;  // the scratch columns are 16-byte aligned and 2^m points long
+        sa.slog = 2 * nm;
+        if (r2c) {
+            sa.out0 = buf[next];
+            sa.out1 = nullptr;
+            sa.out_stride = n;
+        } else {
+            sa.out0 = uo0;
+            sa.out1 = uo1;
+            sa.out_stride = a.out_stride;
+        }
+        sa.t.out0 = sa.out0;
+        const zlfft::SegLaunchFn sfn = t.seg[m - zlfft::kSegMinM][fwd ? 1 : 0][r2c ? ZLFFT_AOS : ol];
+        e = sfn(sa, s, ctx);
+        if (e != cudaSuccess) return cuda_fail(e, "segment launch");
+        if (r2c) {
+            e = p->prec == ZLFFT_F32
+                    ? launch_split<float>(p, dop, out_layout, buf[next], uo0, uo1, nb, a.out_stride, s, ctx)
+                    : launch_split<double>(p, dop, out_layout, buf[next], uo0, uo1, nb, a.out_stride, s, ctx);
+            if (e != cudaSuccess) return cuda_fail(e, "rfft split launch");
+        }
+    }
+    return ZLFFT_OK;
+}
+
+// exec_macro with the plan's scratch: chunks alternate between the plan's two
+// internal streams, forked from and joined back to the caller's stream.
+int exec_macro_planned(zlfft_plan_s* p, int dop, int in_layout, int out_layout, const zlfft::TileArgs& a,
+                       cudaStream_t st, const zlfft::LaunchCtx& ctx) {
+    int rc = ensure_scratch(p);
+    if (rc) return rc;
+    const size_t quarter = p->scratch_bytes / 4;
+    MacroScratch sc{};
+    for (int i = 0; i < 2; ++i) {
+        sc.buf[i][0] = static_cast<char*>(p->d_scratch) + (size_t)i * 2 * quarter;
+        sc.buf[i][1] = sc.buf[i][0] + quarter;
+        sc.stream[i] = p->lanes[i];
+    }
+    sc.chunk = (long long)p->chunk;
+    const long long nchunks = (a.batch + sc.chunk - 1) / sc.chunk;
+    sc.lanes = (nchunks > 1 && p->nlanes > 1) ? 2 : 1;
+    if (sc.lanes > 1) {
+        if (cudaEventRecord(p->ev_fork, st) != cudaSuccess) return fail(ZLFFT_ERR_CUDA, "event record failed");
+        for (int i = 0; i < 2; ++i)
+            if (cudaStreamWaitEvent(p->lanes[i], p->ev_fork, 0) != cudaSuccess)
+                return fail(ZLFFT_ERR_CUDA, "stream wait failed");
+    }
+    rc = exec_macro(p, dop, in_layout, out_layout, a, st, ctx, sc);
+    if (rc) return rc;
+    if (sc.lanes > 1) {
+        for (int i = 0; i < 2; ++i) {
+            if (cudaEventRecord(p->ev_join[i], p->lanes[i]) != cudaSuccess ||
+                cudaStreamWaitEvent(st, p->ev_join[i], 0) != cudaSuccess)
+                return fail(ZLFFT_ERR_CUDA, "stream join failed");
+        }
+    }
+    return ZLFFT_OK;
+}
+
+// The kernels of one prepared device call (prepare_device_call), by size:
+// the macro path, the multi-pass pipeline or one tile kernel launch.
+int dispatch_device(zlfft_plan_s* p, int op, int in_layout, int out_layout, const zlfft::TileArgs& a,
+                    cudaStream_t stream) {
+    const int dop = device_op_code(p, op);
     const int P = p->cfft_order;
     zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
+    if (p->micro >= 0) {
+        DeviceGuard g(p->device);
+        return exec_macro_planned(p, dop, in_layout, out_layout, a, stream, ctx);
+    }
     if (P > zlfft::kTileMaxP && !tile14(p)) {
         DeviceGuard g(p->device);
         return exec_multipass(p, dop, in_layout, out_layout, a, stream, ctx);
@@ -749,6 +936,14 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
     return ZLFFT_OK;
 }
 
+int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,
+                     void* out0, void* out1, size_t batch, size_t in_stride, size_t out_stride, cudaStream_t stream) {
+    zlfft::TileArgs a{};
+    int rc = prepare_device_call(p, op, in_layout, out_layout, in0, in1, out0, out1, batch, in_stride, out_stride, &a);
+    if (rc || batch == 0) return rc;
+    return dispatch_device(p, op, in_layout, out_layout, a, stream);
+}
+
 // ------------------------------------------------------------------ STFT front end
 // Frames f = 0..n_frames-1 of a real signal, frame f = signal[f*hop + n] *
 // window[n] (n < N), each through the RFFT forward (bins or squared
@@ -758,6 +953,8 @@ int exec_device_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, con
 int stft_impl(zlfft_plan_s* p, int op, int out_layout, const void* signal, size_t hop, const void* window,
               void* out0, void* out1, size_t n_frames, size_t out_stride, cudaStream_t stream) {
     if (p->kind != ZLFFT_R2C) return fail(ZLFFT_ERR_INVALID_ARG, "the STFT needs an RFFT plan");
+    if (p->micro >= 0)
+        return fail(ZLFFT_ERR_UNSUPPORTED, "the STFT runs the micro-only form; this plan follows the macro path");
     if (op != ZLFFT_FORWARD && op != ZLFFT_FORWARD_SQR_MAG)
         return fail(ZLFFT_ERR_INVALID_ARG, "STFT op must be FORWARD or FORWARD_SQR_MAG");
     if (out_layout != ZLFFT_AOS && out_layout != ZLFFT_SOA) return fail(ZLFFT_ERR_INVALID_ARG, "invalid layout");
@@ -804,6 +1001,9 @@ int stft_impl(zlfft_plan_s* p, int op, int out_layout, const void* signal, size_
 int istft_impl(zlfft_plan_s* p, int in_layout, const void* in0, const void* in1, size_t in_stride, const void* filter,
                const void* window, size_t hop, size_t n_frames, void* signal, cudaStream_t stream) {
     if (p->kind != ZLFFT_R2C) return fail(ZLFFT_ERR_INVALID_ARG, "the inverse STFT needs an RFFT plan");
+    if (p->micro >= 0)
+        return fail(ZLFFT_ERR_UNSUPPORTED,
+                    "the inverse STFT runs the micro-only form; this plan follows the macro path");
     if (in_layout != ZLFFT_AOS && in_layout != ZLFFT_SOA) return fail(ZLFFT_ERR_INVALID_ARG, "invalid layout");
     const zlfft::IstftTable& t = p->prec == ZLFFT_F32 ? tables().i32 : tables().i64;
     const int pc = p->cfft_order;
@@ -863,26 +1063,36 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 constexpr int kNoAllocMaxDevices = 64;
 struct NoAllocSlot {
-    std::once_flag once;
-    void* ptr = nullptr;
-    cudaError_t err = cudaSuccess;
+    std::mutex mu;
+    void* ptr = nullptr;  // set once the lookup has succeeded
 };
 NoAllocSlot g_noalloc_slots[kNoAllocMaxDevices];
 
 // Device address of the array on `device`. In host code the array's name is
 // only a host-side stand-in, so the address is looked up with
-// cudaGetSymbolAddress, once per device, with that device current.
+// cudaGetSymbolAddress, with that device current, on the first call that
+// succeeds; a failed lookup is reported and tried again by the next call.
 int noalloc_scratch(int device, void** out) {
     if (device < 0 || device >= kNoAllocMaxDevices) return fail(ZLFFT_ERR_INVALID_ARG, "device %d out of range", device);
     NoAllocSlot& slot = g_noalloc_slots[device];
-    std::call_once(slot.once, [&]() {
+    std::lock_guard<std::mutex> lock(slot.mu);
+    if (!slot.ptr) {
         DeviceGuard g(device);
-        slot.err = cudaGetSymbolAddress(&slot.ptr, g_noalloc_scratch);
-        if (slot.err != cudaSuccess) cudaGetLastError();
-    });
-    if (slot.err != cudaSuccess) return cuda_fail(slot.err, "cudaGetSymbolAddress(no-alloc scratch)");
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+        slot.ptr = ptr;
+    }
     *out = slot.ptr;
     return ZLFFT_OK;
+}
+
+// The largest order of the plan's kind and precision whose transform fits
+// one half of the array (an RFFT's inner CFFT is one order below it).
+int noalloc_max_order(const zlfft_plan_s* p) {
+    int o = 0;
+    while ((size_t{1} << (o + 1)) * 2 * p->esize <= kNoAllocScratchBytes / 2) ++o;
+    return p->kind == ZLFFT_R2C ? o + 1 : o;
 }
 
 // The multi-pass orders with the built-in array as the pass intermediates:
@@ -901,8 +1111,8 @@ int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layo
     if (per > half)
         return fail(ZLFFT_ERR_UNSUPPORTED,
                     "one transform needs %zu bytes of intermediate buffer; the allocation-free entry point holds "
-                    "%zu per buffer (order <= %d in this precision)",
-                    per, half, p->esize == 4 ? 22 : 21);
+                    "%zu per buffer (order <= %d for this kind and precision)",
+                    per, half, noalloc_max_order(p));
     void* base = nullptr;
     int rc = noalloc_scratch(p->device, &base);
     if (rc) return rc;
@@ -985,50 +1195,39 @@ int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layo
     return ZLFFT_OK;
 }
 
-// Argument checks of zlfft_exec_device, then the allocation-free dispatch.
+// Argument checks of zlfft_exec_device, then the allocation-free dispatch:
+// the single-CTA sizes run exactly as in zlfft_exec_device (they use no
+// scratch); the multi-pass and macro-path sizes pass their intermediates
+// through the built-in array.
 int exec_device_noalloc_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0,
                              const void* in1, void* out0, void* out1, size_t batch, size_t in_stride,
                              size_t out_stride, cudaStream_t stream) {
-    if (p->cfft_order <= zlfft::kTileMaxP)  // single-CTA orders use no scratch at all
+    if (p->micro < 0 && (p->cfft_order <= zlfft::kTileMaxP || tile14(p)))
         return exec_device_impl(p, op, in_layout, out_layout, in0, in1, out0, out1, batch, in_stride, out_stride,
                                 stream);
-    int rc = validate_op(p, op, in_layout, out_layout);
-    if (rc) return rc;
-    const Extents ex = extents(p, op);
-    const bool in_soa = ex.in_complex && in_layout == ZLFFT_SOA;
-    const bool out_soa = ex.out_complex && out_layout == ZLFFT_SOA;
-    if (!in0 || (in_soa && !in1)) return fail(ZLFFT_ERR_INVALID_ARG, "null input pointer");
-    if (!out0 || (out_soa && !out1)) return fail(ZLFFT_ERR_INVALID_ARG, "null output pointer");
-    if (in_stride == 0) in_stride = ex.in_elems;
-    if (out_stride == 0) out_stride = ex.out_elems;
-    if (batch > 1 && (in_stride < ex.in_elems || out_stride < ex.out_elems))
-        return fail(ZLFFT_ERR_INVALID_ARG, "stride smaller than one transform");
-    const size_t pair = 2 * p->esize;
-    const bool in_pairs = ex.in_complex ? !in_soa : (op != ZLFFT_BACKWARD);
-    const bool out_pairs = ex.out_complex ? !out_soa : (p->kind == ZLFFT_R2C && op == ZLFFT_BACKWARD);
-    if (in_pairs && !aligned(in0, pair)) return fail(ZLFFT_ERR_ALIGNMENT, "input must be %zu-byte aligned", pair);
-    if (out_pairs && !aligned(out0, pair)) return fail(ZLFFT_ERR_ALIGNMENT, "output must be %zu-byte aligned", pair);
-    if (!aligned(in0, p->esize) || (in1 && !aligned(in1, p->esize)) || !aligned(out0, p->esize) ||
-        (out1 && !aligned(out1, p->esize)))
-        return fail(ZLFFT_ERR_ALIGNMENT, "buffers must be aligned to the element type");
-    if (!ex.in_complex && (in_stride % 2)) return fail(ZLFFT_ERR_INVALID_ARG, "RFFT real input stride must be even");
-    if (p->kind == ZLFFT_R2C && op == ZLFFT_BACKWARD && (out_stride % 2))
-        return fail(ZLFFT_ERR_INVALID_ARG, "RFFT real output stride must be even");
-    if (p->kind == ZLFFT_C2C && in0 == out0 && in_layout != out_layout)
-        return fail(ZLFFT_ERR_INVALID_ARG, "in-place transform needs the same layout on both sides");
-    rc = check_aliasing(p, ex, in_soa, out_soa, in0, in1, out0, out1, batch, in_stride, out_stride);
-    if (rc) return rc;
-    if (batch == 0) return ZLFFT_OK;
     zlfft::TileArgs a{};
-    a.in0 = in0;
-    a.in1 = in_soa ? in1 : nullptr;
-    a.out0 = out0;
-    a.out1 = out_soa ? out1 : nullptr;
-    a.batch = (long long)batch;
-    a.in_stride = (long long)(ex.in_complex ? in_stride : in_stride / 2);
-    a.out_stride = (long long)((ex.out_complex || op == ZLFFT_FORWARD_SQR_MAG) ? out_stride : out_stride / 2);
+    int rc = prepare_device_call(p, op, in_layout, out_layout, in0, in1, out0, out1, batch, in_stride, out_stride, &a);
+    if (rc || batch == 0) return rc;
     zlfft::LaunchCtx ctx{p->num_sms, &p->launches};
     DeviceGuard g(p->device);
+    if (p->micro >= 0) {
+        const size_t half = kNoAllocScratchBytes / 2;
+        const size_t per = (size_t{1} << p->cfft_order) * 2 * p->esize;
+        if (per > half)
+            return fail(ZLFFT_ERR_UNSUPPORTED,
+                        "one transform needs %zu bytes of intermediate buffer; the allocation-free entry point "
+                        "holds %zu per buffer (order <= %d for this kind and precision)",
+                        per, half, noalloc_max_order(p));
+        void* base = nullptr;
+        rc = noalloc_scratch(p->device, &base);
+        if (rc) return rc;
+        MacroScratch sc{};
+        sc.buf[0][0] = static_cast<char*>(base);
+        sc.buf[0][1] = sc.buf[0][0] + half;
+        sc.chunk = (long long)(half / per);
+        sc.lanes = 1;
+        return exec_macro(p, device_op_code(p, op), in_layout, out_layout, a, stream, ctx, sc);
+    }
     return exec_multipass_noalloc(p, device_op_code(p, op), in_layout, out_layout, a, stream, ctx);
 }
 
@@ -1558,6 +1757,90 @@ int mixed_graph(zlfft_mixed_s* m, cudaStream_t st) {
     m->launches += m->graph_launches;
     return ZLFFT_OK;
 }
+// ------------------------------------------------------------------ the reference's algorithm switch
+// get_switch_order<F> of the reference (src/common/zldsp_fft_common_system.hpp:132-157)
+// on this host: the same cache queries (sysconf on Linux, with the
+// reference's defaults of 32 KiB L1d, 256 KiB L2 and no L3 where a query
+// gives nothing) and the same arithmetic.
+void host_switch_order(size_t esize, int* max_l1_order, int* switch_order) {
+    auto cache = [](int name, long dflt) -> size_t {
+        const long v = sysconf(name);
+        return (size_t)(v > 0 ? v : dflt);
+    };
+    auto bit_width = [](size_t x) -> int {
+        int w = 0;
+        while (x) {
+            ++w;
+            x >>= 1;
+        }
+        return w;
+    };
+    const size_t l1d = cache(_SC_LEVEL1_DCACHE_SIZE, 32768);
+    const size_t l2 = cache(_SC_LEVEL2_CACHE_SIZE, 262144);
+    const size_t l3 = cache(_SC_LEVEL3_CACHE_SIZE, 0);
+    const size_t l1e = l1d / (8 * esize), l2e = l2 / (12 * esize);
+    const int l1o = l1e == 0 ? 0 : bit_width(l1e) - 1;
+    const int l2o = l2e == 0 ? 0 : bit_width(l2e) - 1;
+    int sw = std::max(l1o + 4, l2o);
+    if (l3 > (size_t{64} << 20)) {
+        const size_t l3e = l3 / (12 * esize);
+        sw = std::max(sw, l3e == 0 ? 0 : bit_width(l3e) - 1);
+    }
+    *max_l1_order = l1o;
+    *switch_order = sw;
+}
+
+// Unified and per-stage twiddle tables of order `order` (the plan's micro
+// order), generated as the plan's own tables are: the bits equal the plan
+// table's entries t * 2^(cfft_order - order).
+int make_micro_tables(zlfft_plan_s* p, int order) {
+    const long long m = 1LL << order;
+    const size_t cx_bytes = 2 * p->esize;
+    const long long cnt = 3 * m / 4;
+    const long long l0 = zlfft::stage_l0(order);
+    const long long scnt = m - l0;
+    if (cudaMalloc(&p->d_mtw, (size_t)(cnt + 1) * cx_bytes) != cudaSuccess)
+        return alloc_fail("micro twiddle", (size_t)(cnt + 1) * cx_bytes);
+    if (cudaMalloc(&p->d_mtws, (size_t)(scnt + 1) * cx_bytes) != cudaSuccess)
+        return alloc_fail("micro stage twiddle", (size_t)(scnt + 1) * cx_bytes);
+    if (p->prec == ZLFFT_F32) {
+        twiddle_kernel<float><<<(unsigned)((cnt + 255) / 256), 256, 0, p->stream>>>(static_cast<float2*>(p->d_mtw),
+                                                                                     order, cnt);
+        stage_table_kernel<float><<<(unsigned)((scnt + 255) / 256), 256, 0, p->stream>>>(
+            static_cast<float2*>(p->d_mtws), static_cast<const float2*>(p->d_mtw), order, scnt);
+    } else {
+        twiddle_kernel<double><<<(unsigned)((cnt + 255) / 256), 256, 0, p->stream>>>(static_cast<double2*>(p->d_mtw),
+                                                                                      order, cnt);
+        stage_table_kernel<double><<<(unsigned)((scnt + 255) / 256), 256, 0, p->stream>>>(
+            static_cast<double2*>(p->d_mtws), static_cast<const double2*>(p->d_mtw), order, scnt);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "micro twiddle generation");
+    return ZLFFT_OK;
+}
+
+// Make a plain plan follow the reference's switch (src/common/zldsp_fft_common_init.hpp:305-339):
+// a CFFT order at or above switch_order takes the macro path with micro order
+// max_l1_order, or max_l1_order - 1 when the difference is odd.
+int apply_switch(zlfft_plan_s* p, int max_l1_order, int switch_order) {
+    p->max_l1 = max_l1_order;
+    p->switch_order = switch_order;
+    const int O = p->cfft_order;
+    if (O < switch_order) return ZLFFT_OK;  // the micro-only path: the plain plan as it is
+    const int m = ((O - max_l1_order) % 2 != 0) ? max_l1_order - 1 : max_l1_order;
+    if (m < zlfft::kSegMinM || m > zlfft::kSegMaxM || O - m < 2)
+        return fail(ZLFFT_ERR_UNSUPPORTED,
+                    "the macro path of CFFT order %d with micro order %d is not built (micro orders %d-%d, at "
+                    "least one macro stage)",
+                    O, m, zlfft::kSegMinM, zlfft::kSegMaxM);
+    DeviceGuard g(p->device);
+    int rc = make_micro_tables(p, m);
+    if (rc) return rc;
+    p->micro = m;
+    return ZLFFT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1571,7 +1854,8 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
     if (order > 30) return fail(ZLFFT_ERR_INVALID_ARG, "order %zu out of range", order);
     if (kind == ZLFFT_R2C && order < 1)
         return fail(ZLFFT_ERR_INVALID_ARG, "RFFT order must be >= 1 (the reference underflows at 0)");
-    if (mode != ZLFFT_MODE_PLAIN && mode != ZLFFT_MODE_TC_FP16 && mode != ZLFFT_MODE_TUNED && mode != ZLFFT_MODE_FAST)
+    if (mode != ZLFFT_MODE_PLAIN && mode != ZLFFT_MODE_TC_FP16 && mode != ZLFFT_MODE_TUNED && mode != ZLFFT_MODE_FAST &&
+        mode != ZLFFT_MODE_HOST)
         return fail(ZLFFT_ERR_UNSUPPORTED, "mode %d not available", mode);
     if (mode == ZLFFT_MODE_TC_FP16 && (kind != ZLFFT_C2C || precision != ZLFFT_F32))
         return fail(ZLFFT_ERR_UNSUPPORTED, "the tensor-core split form is built for CFFT<float>");
@@ -1707,7 +1991,52 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
         release(p);
         return cuda_fail(e, "twiddle generation");
     }
+    if (mode == ZLFFT_MODE_HOST) {
+        int l1o = 0, swo = 0;
+        host_switch_order(p->esize, &l1o, &swo);
+        const int rc = apply_switch(p, l1o, swo);
+        if (rc) {
+            release(p);
+            return rc;
+        }
+    }
     *out = p;
+    return ZLFFT_OK;
+}
+
+int zlfft_plan_create_hybrid(zlfft_plan* out, int kind, int precision, size_t order, int max_l1_order,
+                             int switch_order, int device) {
+    if (!out) return fail(ZLFFT_ERR_INVALID_ARG, "plan pointer is null");
+    *out = nullptr;
+    if (max_l1_order < 0 || max_l1_order > 30 || switch_order < 0)
+        return fail(ZLFFT_ERR_INVALID_ARG, "invalid switch (max_l1_order %d, switch_order %d)", max_l1_order,
+                    switch_order);
+    zlfft_plan p = nullptr;
+    int rc = zlfft_plan_create(&p, kind, precision, order, ZLFFT_MODE_PLAIN, device);
+    if (rc) return rc;
+    rc = apply_switch(p, max_l1_order, switch_order);
+    if (rc) {
+        release(p);
+        return rc;
+    }
+    *out = p;
+    return ZLFFT_OK;
+}
+
+int zlfft_host_switch_order(int precision, size_t* max_l1_order, size_t* switch_order) {
+    if (!max_l1_order || !switch_order) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    if (precision != ZLFFT_F32 && precision != ZLFFT_F64)
+        return fail(ZLFFT_ERR_INVALID_ARG, "invalid precision %d", precision);
+    int l1o = 0, swo = 0;
+    host_switch_order(precision == ZLFFT_F32 ? 4 : 8, &l1o, &swo);
+    *max_l1_order = (size_t)l1o;
+    *switch_order = (size_t)swo;
+    return ZLFFT_OK;
+}
+
+int zlfft_plan_get_micro_order(zlfft_plan plan, int* micro_order) {
+    if (!plan || !micro_order) return fail(ZLFFT_ERR_INVALID_ARG, "null argument");
+    *micro_order = plan->micro;
     return ZLFFT_OK;
 }
 

@@ -149,13 +149,15 @@ __device__ __forceinline__ C cmul_rn(const C x, const C h) {
     return cx<C>(sub_rn(mul_rn(x.x, h.x), mul_rn(x.y, h.y)), add_rn(mul_rn(x.x, h.y), mul_rn(x.y, h.x)));
 }
 
-template <typename F, int P, int OP = kC2CFwd, int BLOCK = 128>
+template <typename F, int P, int OP = kC2CFwd, int BLOCK = 128, int EM = 0>
 struct TileCfg {
     using C = Cx<F>;
     static constexpr int N = 1 << P;
     // points per thread: the largest group radix; order 14 takes two radix-16
-    // butterflies per thread per group (512 threads for 16384 points)
-    static constexpr int E = P == 14 ? 2 * tile_elems(P) : tile_elems(P);
+    // butterflies per thread per group (512 threads for 16384 points); EM > 0
+    // sets it (a multiple of the largest group radix)
+    static constexpr int E = EM > 0 ? EM : (P == 14 ? 2 * tile_elems(P) : tile_elems(P));
+    static_assert(E % tile_elems(P) == 0 || P == 0, "points per thread: a multiple of the largest group radix");
     static constexpr int T = N / E;  // threads per transform
     static constexpr int TPC = T >= BLOCK ? 1 : BLOCK / T;
     static constexpr int THREADS = T * TPC;
@@ -474,10 +476,15 @@ __device__ __forceinline__ void group16_fast(C* r, uint32_t k, const C* tws) {
 // and the processing of one tile. tile_kernel drives it over a contiguous
 // batch with TMA prefetch; mixed_kernel (zlfft_mixed.cuh) drives it over a
 // queue of tiles of many orders.
+//
+// KEEP (forward C2C only): the transform's output stays in the exchange
+// buffer instead of going to global memory, slot-interleaved with an XOR
+// swizzle (keep_idx), for a caller that stores the TPC transforms of a tile
+// together (the transposed store of the macro path, zlfft_macro.cuh).
 template <typename F, int P, int OP, int IL, int OL, int BLOCK = 128, bool GATHER = false, bool WIN = false,
-          bool FAST = false>
+          bool FAST = false, bool KEEP = false, int EM = 0>
 struct TileWorker {
-    using Cfg = TileCfg<F, P, OP, BLOCK>;
+    using Cfg = TileCfg<F, P, OP, BLOCK, EM>;
     using C = Cx<F>;
     static constexpr int N = Cfg::N, E = Cfg::E, T = Cfg::T, TPC = Cfg::TPC, NG = Cfg::NG;
     static constexpr bool kFwd = (OP == kC2CFwd || OP == kR2CFwd || OP == kR2CSqrMag);
@@ -539,6 +546,14 @@ struct TileWorker {
 
     __device__ __forceinline__ uint32_t sidx(int pos) const { return swz<C>(sbase + (uint32_t)pos); }
 
+    // KEEP layout: output k of slot q at k * TPC + (q ^ (k % TPC)). With TPC
+    // slots of 8-byte (FP32) or 16-byte (FP64) points filling a 128-byte row,
+    // a warp's writes of consecutive k by one slot and its reads of whole rows
+    // (all slots of consecutive k) both touch every bank once per row.
+    static __device__ __forceinline__ uint32_t keep_idx(int k, int q) {
+        return (uint32_t)k * TPC + (uint32_t)(q ^ (k & (TPC - 1)));
+    }
+
     // Backward RFFT: issue the cp.async copies of tile t's bins into the
     // staging buffer (all threads share them) and commit them as one group.
     __device__ __forceinline__ void stage_bins(const TileArgs& a, long long t) const {
@@ -576,6 +591,7 @@ struct TileWorker {
     __device__ __forceinline__ void run(const TileArgs& a, long long tile, bool use_tma, Refill&& refill,
                                         const Sink& sink = Sink{}) {
         static_assert(!Sink::kActive || OP == kC2RBwd, "output sinks take backward RFFT samples");
+        static_assert(!KEEP || (OP == kC2CFwd && (TPC & (TPC - 1)) == 0), "KEEP: forward C2C, power-of-two slots");
         const C* stage = Cfg::kTMA1 ? sm : sm + (size_t)TPC * N;
         const long long tr = tile * TPC + slot;
         const bool valid = tr < a.batch;
@@ -865,6 +881,14 @@ struct TileWorker {
                                     __stcs(osq, mul_rn(dc, dc));
                                     __stcs(osq + N, mul_rn(ny, ny));
                                 }
+                            }
+                        } else if constexpr (KEEP) {
+                            __syncthreads();  // every input of the last group is read: the buffer is free
+#pragma unroll
+                            for (int u = 0; u < NB; ++u) {
+                                const int b = b_last + u * T;
+#pragma unroll
+                                for (int s = 0; s < G.R; ++s) sm[keep_idx(b + group_mu(G, s) * G.L, slot)] = v[u * G.R + s];
                             }
                         } else {
 #pragma unroll

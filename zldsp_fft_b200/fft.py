@@ -31,18 +31,41 @@ def _prec(dtype) -> int:
     raise TypeError(f"unsupported dtype {dt}; the reference is instantiated for float and double")
 
 
-class Plan:
-    """A zlfft plan (one transform size, kind, precision and form)."""
+def host_switch_order(dtype=np.float32):
+    """(max_l1_order, switch_order) the reference computes from this host's
+    caches (zlfft_host_switch_order; src/common/zldsp_fft_common_system.hpp:132-157)."""
+    a, b = ctypes.c_size_t(), ctypes.c_size_t()
+    C.check(C.lib().zlfft_host_switch_order(_prec(dtype), ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value
 
-    def __init__(self, kind: int, order: int, dtype=np.float32, mode: int = C.MODE_PLAIN, device: int = -1):
+
+class Plan:
+    """A zlfft plan (one transform size, kind, precision and form).
+
+    ``switch=(max_l1_order, switch_order)`` makes a plain plan follow the
+    reference's algorithm switch with those values (zlfft_plan_create_hybrid):
+    orders at or above switch_order run the reference's macro DIF path."""
+
+    def __init__(self, kind: int, order: int, dtype=np.float32, mode: int = C.MODE_PLAIN, device: int = -1,
+                 switch=None):
         self._lib = C.lib()
         self.kind = kind
         self.order = int(order)
         self.prec = _prec(dtype)
         self.mode = mode
         h = ctypes.c_void_p()
-        C.check(self._lib.zlfft_plan_create(ctypes.byref(h), kind, self.prec, self.order, mode, device))
+        if switch is not None:
+            C.check(self._lib.zlfft_plan_create_hybrid(ctypes.byref(h), kind, self.prec, self.order, int(switch[0]),
+                                                       int(switch[1]), device))
+        else:
+            C.check(self._lib.zlfft_plan_create(ctypes.byref(h), kind, self.prec, self.order, mode, device))
         self.handle = h
+
+    def micro_order(self) -> int:
+        """Micro order of the plan's macro path, -1 on the micro-only path."""
+        v = ctypes.c_int()
+        C.check(self._lib.zlfft_plan_get_micro_order(self.handle, ctypes.byref(v)))
+        return v.value
 
     @property
     def real_dtype(self):
@@ -149,9 +172,11 @@ class CFFT:
 
     forward/backward(in, out) accept the reference's four layout pairings:
     AoS->AoS, AoS->SoA, SoA->AoS, SoA->SoA. backward is the unnormalised
-    inverse (backward(forward(x)) == N * x)."""
+    inverse (backward(forward(x)) == N * x). By default the plan follows the
+    reference's algorithm switch as this host's caches set it
+    (MODE_HOST), so the results are the reference's on this host."""
 
-    def __init__(self, order: int, dtype=np.float32, mode: int = C.MODE_PLAIN):
+    def __init__(self, order: int, dtype=np.float32, mode: int = C.MODE_HOST):
         self._plan = Plan(C.C2C, order, dtype, mode)
         self._n = 1 << int(order)
 
@@ -183,9 +208,10 @@ class RFFT:
 
     forward(real_in, out) writes N/2+1 bins (AoS ndarray or SoA pair);
     backward(in, real_out) is unnormalised (backward(forward(x)) == N/2 * x);
-    forward_sqr_mag(real_in, out) writes N/2+1 squared magnitudes."""
+    forward_sqr_mag(real_in, out) writes N/2+1 squared magnitudes. Like CFFT,
+    it follows the reference's algorithm switch of this host by default."""
 
-    def __init__(self, order: int, dtype=np.float32, mode: int = C.MODE_PLAIN):
+    def __init__(self, order: int, dtype=np.float32, mode: int = C.MODE_HOST):
         self._plan = Plan(C.R2C, order, dtype, mode)
         self._n = 1 << int(order)
         self._nb = self._n // 2 + 1
