@@ -515,3 +515,43 @@ def test_padded_in_place_rfft_and_cross_transform_aliasing_refused():
     with pytest.raises(Z.ZlfftError) as e:
         cplan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, t.data_ptr(), None, t[1].data_ptr(), None, 4)
     assert e.value.code == Z._capi.ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_single_transform_host_path_equals_device_path(oracle, prec):
+    """One small transform from host buffers runs on mapped page-locked
+    buffers (one launch, one synchronisation); it must give the device path's
+    bits in every layout, CFFT orders 0-13 and RFFT orders 1-14, in place too."""
+    ft, ct = (np.float32, np.complex64) if prec == "f32" else (np.float64, np.complex128)
+    rng = np.random.default_rng(1010)
+    for order in range(0, 14):
+        n = 1 << order
+        x = (rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)).astype(ct)
+        cf = Z.CFFT(order, ft)
+        for fwd in (True, False):
+            ref = G.run_c2c(cf.plan, x[None, :], fwd)[0]
+            y = np.zeros_like(x)
+            (cf.forward if fwd else cf.backward)(x, y)
+            assert np.array_equal(y, ref), (order, fwd)
+            re, im = np.zeros(n, ft), np.zeros(n, ft)
+            (cf.forward if fwd else cf.backward)((np.ascontiguousarray(x.real), np.ascontiguousarray(x.imag)),
+                                                 (re, im))
+            assert np.array_equal(re + 1j * im, ref), (order, fwd)
+            z = x.copy()
+            (cf.forward if fwd else cf.backward)(z, z)  # in place
+            assert np.array_equal(z, ref), (order, fwd)
+    for order in range(1, 15):
+        n = 1 << order
+        xr = rng.uniform(-1, 1, n).astype(ft)
+        rf = Z.RFFT(order, ft)
+        X = np.zeros(n // 2 + 1, ct)
+        rf.forward(xr, X)
+        assert np.array_equal(X, G.run_r2c(rf.plan, xr[None, :])[0]), order
+        P = np.zeros(n // 2 + 1, ft)
+        rf.forward_sqr_mag(xr, P)
+        assert np.array_equal(P, G.run_r2c(rf.plan, xr[None, :], sqr_mag=True)[0]), order
+        back = np.zeros(n, ft)
+        rf.backward(X, back)
+        assert np.array_equal(back, G.run_c2r(rf.plan, X[None, :])[0]), order
+        if prec == "f32":
+            assert np.array_equal(X, oracle.rfft_forward_port(xr)), order

@@ -299,6 +299,16 @@ struct zlfft_plan_s {
     void* d_out = nullptr;
     size_t stage_in_bytes = 0, stage_out_bytes = 0;
     cudaEvent_t ev_host = nullptr;  // orders the chunks' transforms across the two staging streams
+    int* h_err = nullptr;           // page-locked copy of the device error word (host path)
+    // single small transforms from host buffers: page-locked buffers mapped into the device's address
+    // space, read and written by the kernel directly (exec_host_small)
+    void* hm_in = nullptr;
+    void* hm_out = nullptr;
+    int* hm_err = nullptr;  // the kernel's error word for those calls, mapped too
+    size_t hm_in_bytes = 0, hm_out_bytes = 0;
+    void* dm_in = nullptr;   // their device addresses
+    void* dm_out = nullptr;
+    void* dm_err = nullptr;
     std::atomic<size_t> launches{0};
     // multi-pass scratch (two buffers of `chunk` transforms each)
     void* d_scratch = nullptr;
@@ -360,6 +370,10 @@ void release(zlfft_plan p) {
     if (p->d_out) cudaFree(p->d_out);
     if (p->h_in) cudaFreeHost(p->h_in);
     if (p->h_out) cudaFreeHost(p->h_out);
+    if (p->h_err) cudaFreeHost(p->h_err);
+    if (p->hm_in) cudaFreeHost(p->hm_in);
+    if (p->hm_out) cudaFreeHost(p->hm_out);
+    if (p->hm_err) cudaFreeHost(p->hm_err);
     if (p->stream) cudaStreamDestroy(p->stream);
     if (p->stream2) cudaStreamDestroy(p->stream2);
     delete p;
@@ -1234,6 +1248,11 @@ int exec_device_noalloc_impl(zlfft_plan_s* p, int op, int in_layout, int out_lay
 int ensure_staging(zlfft_plan_s* p, size_t in_bytes, size_t out_bytes) {
     if (!p->ev_host && cudaEventCreateWithFlags(&p->ev_host, cudaEventDisableTiming) != cudaSuccess)
         return fail(ZLFFT_ERR_CUDA, "event creation failed");
+    if (!p->h_err) {
+        if (cudaMallocHost(reinterpret_cast<void**>(&p->h_err), sizeof(int)) != cudaSuccess)
+            return alloc_fail("staging", sizeof(int));
+        *p->h_err = 0;
+    }
     if (in_bytes > p->stage_in_bytes) {
         if (p->h_in) cudaFreeHost(p->h_in);
         if (p->d_in) cudaFree(p->d_in);
@@ -1264,6 +1283,82 @@ bool is_pinned(const void* ptr) {
     return at.type == cudaMemoryTypeHost;
 }
 
+// Single small transforms from host buffers: the reference's own call
+// pattern (one transform per call, often from an audio thread). Copies
+// queued around the kernel cost more than the transform, so the kernel reads
+// its input from, and writes its output to, page-locked host buffers mapped
+// into the device's address space: a call copies the caller's input into the
+// mapped buffer, launches one kernel, synchronises the plan's stream once and
+// copies the output out. The kernel's error word is mapped as well, so no
+// separate read-back is queued. Inputs are read with plain loads (no bulk
+// copies from host memory). ZLFFT_HOST_ZEROCOPY=0 turns the path off
+// (comparison with the staged path).
+constexpr size_t kSmallHostBytes = 256 << 10;  // in + out bytes of one transform, at most
+
+bool small_host_call(const zlfft_plan_s* p, size_t batch, size_t in_bytes, size_t out_bytes) {
+    static const bool enabled = [] {
+        const char* e = getenv("ZLFFT_HOST_ZEROCOPY");
+        return !(e && e[0] == '0');
+    }();
+    return enabled && batch == 1 && p->micro < 0 && p->cfft_order <= zlfft::kTileMaxP &&
+           in_bytes + out_bytes <= kSmallHostBytes;
+}
+
+int ensure_mapped(zlfft_plan_s* p, size_t in_bytes, size_t out_bytes) {
+    auto grow = [](void** buf, size_t* have, size_t want) -> bool {
+        if (want <= *have) return true;
+        if (*buf) cudaFreeHost(*buf);
+        *buf = nullptr;
+        *have = 0;
+        if (cudaHostAlloc(buf, want, cudaHostAllocMapped) != cudaSuccess) return false;
+        *have = want;
+        return true;
+    };
+    if (!grow(&p->hm_in, &p->hm_in_bytes, in_bytes) || !grow(&p->hm_out, &p->hm_out_bytes, out_bytes))
+        return alloc_fail("mapped staging", in_bytes + out_bytes);
+    if (!p->hm_err) {
+        if (cudaHostAlloc(reinterpret_cast<void**>(&p->hm_err), sizeof(int), cudaHostAllocMapped) != cudaSuccess)
+            return alloc_fail("mapped error word", sizeof(int));
+        *p->hm_err = 0;
+    }
+    ZL_CUDA(cudaHostGetDevicePointer(&p->dm_in, p->hm_in, 0));
+    ZL_CUDA(cudaHostGetDevicePointer(&p->dm_out, p->hm_out, 0));
+    ZL_CUDA(cudaHostGetDevicePointer(&p->dm_err, p->hm_err, 0));
+    return ZLFFT_OK;
+}
+
+int exec_host_small(zlfft_plan_s* p, int op, int in_layout, int out_layout, const void* in0, const void* in1,
+                    void* out0, void* out1, size_t in_part, size_t out_part, int in_parts, int out_parts) {
+    if (in_part * in_parts > p->hm_in_bytes || out_part * out_parts > p->hm_out_bytes || !p->hm_err) {
+        const int rc0 = ensure_mapped(p, in_part * in_parts, out_part * out_parts);
+        if (rc0) return rc0;
+    }
+    memcpy(p->hm_in, in0, in_part);
+    if (in_parts == 2) memcpy(static_cast<char*>(p->hm_in) + in_part, in1, in_part);
+    char* di = static_cast<char*>(p->dm_in);
+    char* dd = static_cast<char*>(p->dm_out);
+    zlfft::TileArgs a{};
+    int rc = prepare_device_call(p, op, in_layout, out_layout, di, in_parts == 2 ? di + in_part : nullptr, dd,
+                                 out_parts == 2 ? dd + out_part : nullptr, 1, 0, 0, &a);
+    if (rc) return rc;
+    a.tma = 0;
+    a.err = static_cast<int*>(p->dm_err);
+    rc = dispatch_device(p, op, in_layout, out_layout, a, p->stream);
+    if (rc) {
+        cudaStreamSynchronize(p->stream);
+        return rc;
+    }
+    ZL_CUDA(cudaStreamSynchronize(p->stream));
+    const int e = *static_cast<volatile int*>(p->hm_err);
+    if (e) {
+        *p->hm_err = 0;
+        return fail(ZLFFT_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration limit (code %d)", e);
+    }
+    memcpy(out0, p->hm_out, out_part);
+    if (out_parts == 2) memcpy(out1, static_cast<char*>(p->hm_out) + out_part, out_part);
+    return ZLFFT_OK;
+}
+
 // Host-pointer path: H2D copy of the input (directly from the caller's
 // buffer when it is page-locked, else through the plan's pinned staging),
 // the device kernel on the plan's stream, D2H copy back, synchronise.
@@ -1286,6 +1381,9 @@ int exec_host_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const
     const size_t in_bytes = in_part * in_parts * batch, out_bytes = out_part * out_parts * batch;
     std::lock_guard<std::mutex> lock(p->mu);
     DeviceGuard g(p->device);
+    if (small_host_call(p, batch, in_bytes, out_bytes))
+        return exec_host_small(p, op, in_layout, out_layout, in0, in1, out0, out1, in_part, out_part, in_parts,
+                               out_parts);
     const bool pin_in = is_pinned(in0) && (!in_soa || is_pinned(in1));
     const bool pin_out = is_pinned(out0) && (!out_soa || is_pinned(out1));
     rc = ensure_staging(p, in_bytes, out_bytes);
@@ -1340,15 +1438,19 @@ int exec_host_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const
             if (e != cudaSuccess) return drain(cuda_fail(e, "cudaMemcpyAsync (D2H)"));
         }
     }
+    // the error word comes back behind the last chunk's transform (the
+    // chunks' transforms are ordered by ev_host), with the output copies
+    {
+        const cudaStream_t last = ss[(int)(((batch + chunk - 1) / chunk - 1) & 1)];
+        const cudaError_t e = cudaMemcpyAsync(p->h_err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, last);
+        if (e != cudaSuccess) return drain(cuda_fail(e, "cudaMemcpyAsync (error word)"));
+    }
     ZL_CUDA(cudaStreamSynchronize(ss[0]));
     ZL_CUDA(cudaStreamSynchronize(ss[1]));
-    {
-        int derr = 0;
-        ZL_CUDA(cudaMemcpy(&derr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (derr) {
-            cudaMemset(p->d_err, 0, sizeof(int));
-            return fail(ZLFFT_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration limit (code %d)", derr);
-        }
+    if (const int derr = *static_cast<volatile int*>(p->h_err)) {
+        *p->h_err = 0;
+        cudaMemset(p->d_err, 0, sizeof(int));
+        return fail(ZLFFT_ERR_DEVICE_TIMEOUT, "a device-side wait ran out of its iteration limit (code %d)", derr);
     }
     if (!pin_out) {
         for (int q = 0; q < out_parts; ++q)
