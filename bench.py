@@ -227,6 +227,39 @@ class ClockSampler:
                 "samples": len(self.samples), "power_w_max": max(pw) if pw else None}
 
 
+def host_info():
+    """The CPU a baseline runs on: model, hardware threads, cache sizes, and the
+    reference's algorithm switch there (get_switch_order<F>,
+    src/common/zldsp_fft_common_system.hpp:132-157), which decides whether the
+    reference timed its micro-only Stockham path or its macro DIF path."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    caches = {}
+    for key, name in (("l1d_bytes", "SC_LEVEL1_DCACHE_SIZE"), ("l2_bytes", "SC_LEVEL2_CACHE_SIZE"),
+                      ("l3_bytes", "SC_LEVEL3_CACHE_SIZE")):
+        try:
+            caches[key] = os.sysconf(name)
+        except (ValueError, OSError):
+            caches[key] = None
+    switch = {}
+    try:
+        from oracle import oracle as O
+        for prec in ("f32", "f64"):
+            l1, sw = O.ref_switch_order(prec) if O.ref_available() else (None, None)
+            switch[prec] = {"max_l1_order": l1, "switch_order": sw,
+                            "source": "the reference's own code" if O.ref_available() else "unavailable"}
+    except Exception as e:  # reported, never required
+        switch = {"error": str(e)[:120]}
+    return {"cpu_model": model, "hw_threads": os.cpu_count(), **caches, "reference_switch_order": switch}
+
+
 # ------------------------------------------------------------------ workloads
 def hann_frames(b, n, seed):
     """3 sinusoids (f ~ U(0, 0.5) cycles/sample, A ~ U[0.1, 1], phase ~ U[0, 2pi))
@@ -262,7 +295,6 @@ class Rfft12:
             "r2c_sqr_mag": b * (4 * n + 4 * nb),
         }
         self.bytes_per_step = sum(self.op_bytes.values())
-        self.dominant = "r2c_fwd_aos"
 
     # ---- GPU (ours)
     def setup(self, device):
@@ -307,7 +339,7 @@ class Rfft12:
         return self.plan.take_launch_count()
 
     def cpu_sample_desc(self, frames):
-        return f"{frames} of {self.batch} frames, same ops as one step, median of 3"
+        return f"{frames} of {self.batch} frames, same ops as one step"
 
     # ---- end to end through the host API (pinned host buffers)
     def setup_e2e(self):
@@ -374,7 +406,6 @@ class Cfft2G:
             for d in ("fwd", "bwd"):
                 self.op_bytes[f"c2c_{d}_order{o}"] = 2 * 8 * self.total  # read + write
         self.bytes_per_step = sum(self.op_bytes.values())
-        self.dominant = "c2c_fwd_order16"
 
     def setup(self, device):
         import torch
@@ -421,10 +452,17 @@ class Cfft2G:
         import torch
         Z = self.Z
         out = {}
-        for form, mode in (("plain", Z.MODE_PLAIN), ("fast", Z.MODE_FAST), ("tc_fp16", Z.MODE_TC_FP16)):
+        # "macro": the reference's own algorithm on a small-cache host (its switch at order 14 with
+        # micro order 10: DIF macro stages + per-segment Stockham + transposed store), bit-identical
+        # to the reference built there
+        for form, mode in (("plain", Z.MODE_PLAIN), ("fast", Z.MODE_FAST), ("tc_fp16", Z.MODE_TC_FP16),
+                           ("macro", None)):
             res = {}
             for o in self.orders:
-                p = Z.Plan(Z.C2C, o, np.float32, mode=mode, device=self.A.device.index)
+                if mode is None:
+                    p = Z.Plan(Z.C2C, o, np.float32, device=self.A.device.index, switch=(10, 14))
+                else:
+                    p = Z.Plan(Z.C2C, o, np.float32, mode=mode, device=self.A.device.index)
                 b = self.total >> o
 
                 def step():
@@ -451,6 +489,9 @@ class Cfft2G:
                 res[f"order{o}"] = {"gbs": round(2 * 16 * self.total / (ms / 1e3) / 1e9, 1),
                                     "max_rel_l2": float(err.max()), "tolerance": 4 * o * 2.0 ** -24}
             out[form] = res
+        out["macro_host_switch"] = {"max_l1_order": 10, "switch_order": 14,
+                                    "what": "the reference's macro path as a host with a 48 KiB L1d, 1 MiB L2 and "
+                                            "no L3 runs it"}
         if self.tuning is not None:
             out["autotuned_plans"] = self.tuning
         return out
@@ -460,7 +501,7 @@ class Cfft2G:
     def cpu_sample_desc(self, frames):
         cnt = [max(1, min(frames >> max(0, o - 14), self.total >> o)) for o in self.orders]
         return (f"forward+backward of {cnt[0]}/{cnt[1]}/{cnt[2]} transforms of orders 14/16/20 "
-                f"(of 16384/4096/256 per step), median of 3")
+                f"(of 16384/4096/256 per step)")
 
     def setup_e2e(self):
         import torch
@@ -535,7 +576,6 @@ class Mixed:
         self.out_total = int(up(self.out_sz).sum())
         self.bytes_per_step = int(self.in_sz.sum() + self.out_sz.sum())
         self.op_bytes = {"mixed_graph": self.bytes_per_step}
-        self.dominant = "mixed_graph"
         self.batch = self.count
         self.host_in = None
 
@@ -611,7 +651,7 @@ class Mixed:
         return out
 
     def cpu_sample_desc(self, frames):
-        return f"the first {frames} of the 20,000 transforms, grouped by (kind, order), median of 3"
+        return f"the first {frames} of the 20,000 transforms, grouped by (kind, order)"
 
     e2e_slices = 4
     e2e_api = ("zlfft_exec_mixed_device on 4 slices of the batch (a MixedBatch each, graph schedule), "
@@ -692,12 +732,12 @@ class Cfft64:
     l2 = "each op reads 512 MiB and writes 512 MiB, > 4x L2 (no L2 flush needed)"
     order, batch = 16, 512
     dtype = "f64"
+    form = "tuned"
 
     def __init__(self):
         n = 1 << self.order
         self.op_bytes = {"c2c_f64_fwd": 2 * 16 * n * self.batch, "c2c_f64_bwd": 2 * 16 * n * self.batch}
         self.bytes_per_step = sum(self.op_bytes.values())
-        self.dominant = "c2c_f64_fwd"
         self.host_in = None
 
     def setup(self, device):
@@ -707,7 +747,6 @@ class Cfft64:
         n = 1 << self.order
         Z.autotune(Z.C2C, self.order, self.order, np.float64, device=device)  # set-up: per-order plan choice
         self.tuning = Z.tuning(Z.C2C, self.order, np.float64, device=device)
-        self.form = "tuned"
         self.plan = Z.Plan(Z.C2C, self.order, np.float64, mode=Z.MODE_TUNED, device=device)
         g = torch.Generator(device=device)
         g.manual_seed(1005)
@@ -768,7 +807,7 @@ class Cfft64:
         }
 
     def cpu_sample_desc(self, frames):
-        return f"forward+backward of {frames} of the 512 transforms, median of 3"
+        return f"forward+backward of {frames} of the 512 transforms"
 
     def setup_e2e(self):
         import torch
@@ -821,7 +860,6 @@ class Cfft10:
         n = 1 << self.order
         self.op_bytes = {"c2c_fwd_bwd": 32 * n}
         self.bytes_per_step = sum(self.op_bytes.values())
-        self.dominant = "c2c_fwd_bwd"
         self.host_in = None
 
     def setup(self, device):
@@ -892,20 +930,24 @@ class Cfft10:
         }
 
     def cpu_sample_desc(self, frames):
-        return f"{frames} repetitions of the single forward+backward transform in one call, one thread, median of 3"
+        return f"{frames} repetitions of the single forward+backward transform in one call, one thread"
+
+    e2e_steps = 2000  # forward + backward pairs timed through the drop-in class
+    e2e_api = ("zldsp::fft::CFFT<float>(10).forward then .backward on host numpy buffers (the drop-in "
+               "class, ZLFFT_MODE_HOST): one transform per call, synchronous, as the reference's callers make them")
 
     def setup_e2e(self):
-        import torch
         n = 1 << self.order
-        self.hA = torch.from_numpy(self.host_x.view(np.float32).copy()).pin_memory()
-        self.hB = torch.empty_like(self.hA).pin_memory()
+        self.cf = self.Z.CFFT(self.order, np.float32)
+        self.hx = self.host_x.copy()
+        self.hy = np.empty_like(self.hx)
+        self.hz = np.empty_like(self.hx)
         self.e2e_h2d = 2 * 8 * n
         self.e2e_d2h = 2 * 8 * n
 
     def e2e_step(self):
-        Z, p = self.Z, self.plan
-        p.exec_host(Z.FORWARD, Z.AOS, Z.AOS, self.hA.data_ptr(), None, self.hB.data_ptr(), None, 1)
-        p.exec_host(Z.BACKWARD, Z.AOS, Z.AOS, self.hB.data_ptr(), None, self.hB.data_ptr(), None, 1)
+        self.cf.forward(self.hx, self.hy)
+        self.cf.backward(self.hy, self.hz)
 
     def cpu_run(self, frames, threads, kind):
         from oracle import oracle as O
@@ -952,7 +994,6 @@ class Stft:
         self.nb = n // 2 + 1
         self.op_bytes = {"stft_sqr_mag": 4 * self.total + 4 * self.nb * self.nf}
         self.bytes_per_step = self.op_bytes["stft_sqr_mag"]
-        self.dominant = "stft_sqr_mag"
         self.batch = self.nf
         self.host_in = None
 
@@ -1009,7 +1050,7 @@ class Stft:
                 "fused_equals_unfused_bitwise": bool(torch.equal(self.out, ref_out))}
 
     def cpu_sample_desc(self, frames):
-        return f"{frames} of {self.nf} frames: numpy framing + window, then the reference's forward_sqr_mag, median of 3"
+        return f"{frames} of {self.nf} frames: numpy framing + window, then the reference's forward_sqr_mag"
 
     e2e_slices = 8
     e2e_api = ("zlfft_stft_device on 8 slices of the frames, pinned host buffers, each slice's new signal "
@@ -1091,7 +1132,6 @@ class Istft:
         self.nb = n // 2 + 1
         self.op_bytes = {"istft_filter_window": 8 * self.nb * self.nf + 4 * self.total}
         self.bytes_per_step = self.op_bytes["istft_filter_window"]
-        self.dominant = "istft_filter_window"
         self.batch = self.nf
         self.host_in = None
 
@@ -1172,7 +1212,7 @@ class Istft:
 
     def cpu_sample_desc(self, frames):
         return (f"{frames} of {self.nf} frames: numpy filter multiply, the reference's RFFT backward, numpy window "
-                f"and sequential overlap-add, median of 3")
+                f"and sequential overlap-add")
 
     e2e_slices = 8
     e2e_api = ("zlfft_istft_device on 8 slices of the frames (each also given the K - 1 frames before it, "
@@ -1249,25 +1289,49 @@ WORKLOADS = {"rfft12": Rfft12, "cfft2g": Cfft2G, "mixed": Mixed, "cfft64": Cfft6
 
 
 # ------------------------------------------------------------------ CPU baseline
-def cpu_baseline(wl, target_s=3.0, threads=None, kind=None):
-    from oracle import oracle as O
-    if kind is None:
-        kind = "reference" if O.ref_available() else "port"
-    threads = threads or getattr(wl, "cpu_threads", None) or (os.cpu_count() or 1) if kind == "reference" else 1
-    frames = 64
+CPU_SAMPLE_S = 1.0     # seconds of CPU work per sample (the baseline takes the median of 3)
+CPU_FRAMES_CAP = 2048  # rfft12: frames generated for the CPU sample
+
+
+def cpu_sample_frames(wl, threads, kind, target_s=CPU_SAMPLE_S):
+    """The one sampling rule of both CPU figures (the cpu_baseline of the GPU
+    arm and every step of the reference arm): from 16 transforms (or frames),
+    doubled until one sample takes target_s or covers the workload."""
     avail = getattr(wl, "batch_for_cpu", wl.batch) if wl.host_in is None else wl.host_in.shape[0]
-    nbytes, dt = wl.cpu_run(frames, threads, kind)
-    while dt < target_s / 4 and frames < avail:
-        frames = min(avail, frames * 4)
-        nbytes, dt = wl.cpu_run(frames, threads, kind)
-    runs = [(nbytes, dt)]
-    for _ in range(2):
-        runs.append(wl.cpu_run(frames, threads, kind))
+    frames = 16
+    _, dt = wl.cpu_run(frames, threads, kind)
+    while dt < target_s and frames < avail:
+        frames = min(avail, frames * 2)
+        _, dt = wl.cpu_run(frames, threads, kind)
+    return frames
+
+
+def cpu_threads_kind(wl):
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    threads = (getattr(wl, "cpu_threads", None) or os.cpu_count() or 1) if kind == "reference" else 1
+    return threads, kind
+
+
+def cpu_baseline(wl):
+    threads, kind = cpu_threads_kind(wl)
+    if hasattr(wl, "n") and wl.host_in is not None:
+        wl.host_in = wl.host_in[:CPU_FRAMES_CAP]
+    frames = cpu_sample_frames(wl, threads, kind)
+    runs = [wl.cpu_run(frames, threads, kind) for _ in range(3)]
     gbs = statistics.median(b / t / 1e9 for b, t in runs)
     return {
         "value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-        "sample": wl.cpu_sample_desc(frames),
+        "sample": wl.cpu_sample_desc(frames) + ", median of 3 samples", "host": host_info(),
     }
+
+
+def config_of(wl, world):
+    """The config object of both arms' lines (identical keys and values)."""
+    return {"workload": wl.desc,
+            "form": FORMS.get(getattr(wl, "form", "plain"), FORMS["plain"]),
+            "l2": getattr(wl, "l2", "rotating input/output sets, each step > 2x L2 (no L2 flush needed)"),
+            "parallelism": f"replicas x{world}"}
 
 
 # ------------------------------------------------------------------ arms
@@ -1276,17 +1340,11 @@ def run_reference_arm(args, wl_cls):
     if rank != 0:
         return 0
     wl = wl_cls()
-    from oracle import oracle as O
-    kind = "reference" if O.ref_available() else "port"
-    threads = getattr(wl, "cpu_threads", None) or os.cpu_count() or 1
-    wl.host_in = hann_frames(min(wl.batch, 2048), wl.n, 1002) if hasattr(wl, "n") else None
-    avail = wl.host_in.shape[0] if wl.host_in is not None else getattr(wl, "batch_for_cpu", wl.batch)
-    # each step: a bounded sample of the workload on all host cores
-    frames = 16
-    _, dt = wl.cpu_run(frames, threads, kind)
-    while dt < 0.25 and frames < avail:
-        frames = min(avail, frames * 2)
-        _, dt = wl.cpu_run(frames, threads, kind)
+    threads, kind = cpu_threads_kind(wl)
+    wl.host_in = hann_frames(min(wl.batch, CPU_FRAMES_CAP), wl.n, 1002) if hasattr(wl, "n") else None
+    # each step: a bounded sample of the workload on all host cores, sized by
+    # the same rule as the GPU arm's cpu_baseline
+    frames = cpu_sample_frames(wl, threads, kind)
     for _ in range(args.warmup):
         wl.cpu_run(frames, threads, kind)
     tot_b, tot_t = 0.0, 0.0
@@ -1299,9 +1357,9 @@ def run_reference_arm(args, wl_cls):
         "metric": METRIC, "value": round(v, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * tot_t / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic",
-        "config": {"workload": wl.desc},
+        "config": config_of(wl, args.gpus),
         "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-                         "sample": wl.cpu_sample_desc(frames) + " per step"},
+                         "sample": wl.cpu_sample_desc(frames) + " per step", "host": host_info()},
         "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -1372,7 +1430,7 @@ def run_ours(args, wl_cls):
 
     # end to end through the host API, pinned host buffers, copies inside the region
     wl.setup_e2e()
-    e2e_steps = max(3, min(args.steps, 10))
+    e2e_steps = getattr(wl, "e2e_steps", max(3, min(args.steps, 10)))
     wl.e2e_step()
     barrier()
     t0 = time.perf_counter()
@@ -1387,25 +1445,23 @@ def run_ours(args, wl_cls):
     schedules = wl.compare(stream, max(3, min(args.steps, 10))) if hasattr(wl, "compare") else None
 
     peak, peak_kind = measured_hbm_peak()
-    dom = wl.dominant
+    dom = max(per_op_ms, key=per_op_ms.get)  # the op with the largest share of the step's time
     achieved = wl.op_bytes[dom] / (per_op_ms[dom] / 1e3) / 1e9
     traffic = ncu_traffic(dom)
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic",
-        "config": {"workload": wl.desc,
-                   "form": FORMS.get(getattr(wl, "form", "plain"), FORMS["plain"]),
-                   "l2": getattr(wl, "l2", "rotating input/output sets, each step > 2x L2 (no L2 flush needed)"),
-                   "parallelism": f"replicas x{world}"},
+        "config": config_of(wl, world),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "kernel": dom, "algorithmic_bytes_per_launch": wl.op_bytes[dom],
+                     "kernel": dom, "time_share": round(per_op_ms[dom] / sum(per_op_ms.values()), 3),
+                     "algorithmic_bytes_per_launch": wl.op_bytes[dom],
                      "traffic": traffic},
         "per_op_gbs": {k: round(wl.op_bytes[k] / (v / 1e3) / 1e9, 1) for k, v in per_op_ms.items()},
         "per_op_us": {k: round(v * 1e3, 2) for k, v in per_op_ms.items()},
         "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": wl.e2e_h2d,
-                "d2h_bytes_per_step": wl.e2e_d2h,
+                "d2h_bytes_per_step": wl.e2e_d2h, "us_per_step": round(e2e_s / e2e_steps * 1e6, 2),
                 "api": getattr(wl, "e2e_api", "zlfft_exec_host_batched, pinned host buffers"),
                 "pcie_gbs": pcie, "pcie_bound": round(bound, 2) if bound else None,
                 "frac_of_pcie_bound": round(e2e_val / bound, 3) if bound else None},
