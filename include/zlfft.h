@@ -198,25 +198,26 @@ ZLFFT_API int zlfft_istft_device(zlfft_plan plan, int in_layout, const void* in0
 
 /* As zlfft_exec_device, for callers that cannot allocate device memory when
  * they run a transform: a real-time audio thread (an allocation can block
- * for an unbounded time), work being captured into a CUDA graph (cudaMalloc
- * is not allowed during capture), or a host whose device memory is all
- * handed to its own pool. No reference counterpart: the reference allocates
- * everything in its constructors.
+ * for an unbounded time, and a missed deadline is an audible glitch), or a
+ * host whose device memory is all handed to its own pool. No reference
+ * counterpart: the reference allocates everything in its constructors.
  *
- * Orders 14 and up pass their intermediates through a scratch array built
- * into the library (64 MiB of device memory, reserved on every GPU that loads
- * the library and held until the process exits), instead of the plan's
- * scratch that zlfft_exec_device allocates on first use. This call allocates
- * nothing and creates no streams or events; orders <= 13 need no scratch and
- * run exactly as in zlfft_exec_device. Results are identical to
- * zlfft_exec_device's.
- *  - Limit: one transform must fit one 32 MiB half of the array (FP32 order
- *    <= 22, FP64 order <= 21); larger orders are rejected with
- *    ZLFFT_ERR_UNSUPPORTED.
- *  - The first call on each device looks up the array's device address
- *    (cudaGetSymbolAddress), which may make the driver load the library's
- *    device code; make that first call during set-up, before any stream
- *    capture or real-time section.
+ * Multi-pass orders (complex order 14 and up, except the FP32 CFFT of order
+ * 14 and the FP32 RFFT of order 15, which run one tile per transform) and
+ * plans on the reference's macro path pass their intermediates through a
+ * scratch array built into the library (64 MiB of device memory, reserved on
+ * every GPU that loads the library and held until the process exits), instead
+ * of the plan's scratch that zlfft_exec_device allocates on first use. This
+ * call allocates nothing and creates no streams or events; the other sizes
+ * need no scratch and run exactly as in zlfft_exec_device. Results are
+ * identical to zlfft_exec_device's.
+ *  - Limit: one transform must fit one 32 MiB half of the array: CFFT order
+ *    <= 22 (FP32) / 21 (FP64), RFFT order <= 23 (FP32) / 22 (FP64); larger
+ *    orders are rejected with ZLFFT_ERR_UNSUPPORTED.
+ *  - The first call on each device that needs the array looks up its device
+ *    address (cudaGetSymbolAddress), which may make the driver load the
+ *    library's device code; make that first call during set-up, before any
+ *    real-time section. A failed lookup is reported and retried next call.
  *  - Every call shares the one array and leaves its contents behind (nothing
  *    in it needs to start at zero). Calls whose work overlaps on the GPU
  *    (different streams, or different plans at once) race on it: serialise

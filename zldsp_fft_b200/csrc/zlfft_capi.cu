@@ -1066,7 +1066,6 @@ int istft_impl(zlfft_plan_s* p, int in_layout, const void* in0, const void* in1,
 // ------------------------------------------------------------------ allocation-free execution
 // Some callers cannot allocate device memory at the moment they run a
 // transform: a real-time audio callback must not block on the allocator,
-// work recorded into a CUDA graph must not call cudaMalloc during capture,
 // and hosts that hand the whole device to a memory pool get no memory
 // outside it. Orders 14 and up need intermediate buffers between their
 // passes, which zlfft_exec_device allocates on first use. For those callers
