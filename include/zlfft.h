@@ -62,8 +62,7 @@ typedef struct zlfft_plan_s* zlfft_plan;
 /* computation form */
 #define ZLFFT_MODE_PLAIN 0   /* reference's Stockham radix-4/8 DIT on CUDA cores */
 #define ZLFFT_MODE_TC_FP16 1 /* radix-16 sub-DFTs on tensor cores, split hi/lo FP16 */
-#define ZLFFT_MODE_TC_BF16 2 /* split 3-way BF16 */
-#define ZLFFT_MODE_TC_TF32 3 /* 3xTF32 */
+/* (2 and 3 are not used) */
 #define ZLFFT_MODE_TUNED 4   /* the autotuned plan of this device and size (see zlfft_autotune) */
 #define ZLFFT_MODE_FAST 5    /* plain CUDA-core form whose multi-pass radix-16 groups build their
                                 twiddles from two table values (fewer loads): within the FP bar,

@@ -82,7 +82,7 @@ def test_tc_mode_rejected_where_not_built():
     lib = Z._capi.lib()
     assert lib.zlfft_plan_create(ctypes.byref(h), Z.R2C, Z.F32, 12, Z.MODE_TC_FP16, -1) == Z._capi.ERR_UNSUPPORTED
     assert lib.zlfft_plan_create(ctypes.byref(h), Z.C2C, Z.F64, 16, Z.MODE_TC_FP16, -1) == Z._capi.ERR_UNSUPPORTED
-    assert lib.zlfft_plan_create(ctypes.byref(h), Z.C2C, Z.F32, 16, Z.MODE_TC_BF16, -1) == Z._capi.ERR_UNSUPPORTED
+    assert lib.zlfft_plan_create(ctypes.byref(h), Z.C2C, Z.F32, 16, 2, -1) == Z._capi.ERR_UNSUPPORTED  # no such mode
 
 
 @pytest.mark.parametrize("prec,ft,ct", [("f32", np.float32, np.complex64), ("f64", np.float64, np.complex128)])

@@ -8,15 +8,15 @@ Layers:
   zldsp_fft_b200/fft.py           Python mirror of the reference's classes
 """
 from . import _capi
-from ._capi import (AOS, BACKWARD, C2C, F32, F64, FORWARD, FORWARD_SQR_MAG, MODE_PLAIN, MODE_TC_BF16,
-                    MODE_FAST, MODE_HOST, MODE_TC_FP16, MODE_TC_TF32, MODE_TUNED, R2C, SCHED_GRAPH, SCHED_PER_ORDER,
+from ._capi import (AOS, BACKWARD, C2C, F32, F64, FORWARD, FORWARD_SQR_MAG, MODE_PLAIN,
+                    MODE_FAST, MODE_HOST, MODE_TC_FP16, MODE_TUNED, R2C, SCHED_GRAPH, SCHED_PER_ORDER,
                     SCHED_PERSISTENT, SOA, ZlfftError)
 from .fft import (CFFT, RFFT, MixedBatch, Plan, autotune, host_switch_order, tuning, tuning_clear, tuning_load,
                   tuning_save)
 
 __all__ = [
     "CFFT", "RFFT", "Plan", "MixedBatch", "ZlfftError", "AOS", "SOA", "C2C", "R2C", "F32", "F64", "FORWARD", "BACKWARD",
-    "FORWARD_SQR_MAG", "MODE_PLAIN", "MODE_TC_FP16", "MODE_TC_BF16", "MODE_TC_TF32", "MODE_TUNED", "MODE_FAST",
+    "FORWARD_SQR_MAG", "MODE_PLAIN", "MODE_TC_FP16", "MODE_TUNED", "MODE_FAST",
     "MODE_HOST", "SCHED_PER_ORDER", "SCHED_PERSISTENT", "SCHED_GRAPH", "autotune", "host_switch_order", "tuning",
     "tuning_save", "tuning_load", "tuning_clear",
 ]

@@ -26,7 +26,7 @@ C2C, R2C = 0, 1
 F32, F64 = 0, 1
 AOS, SOA = 0, 1
 FORWARD, BACKWARD, FORWARD_SQR_MAG = 0, 1, 2
-MODE_PLAIN, MODE_TC_FP16, MODE_TC_BF16, MODE_TC_TF32, MODE_TUNED, MODE_FAST, MODE_HOST = 0, 1, 2, 3, 4, 5, 6
+MODE_PLAIN, MODE_TC_FP16, MODE_TUNED, MODE_FAST, MODE_HOST = 0, 1, 4, 5, 6
 SCHED_PER_ORDER, SCHED_PERSISTENT, SCHED_GRAPH = 0, 1, 2
 
 
