@@ -936,6 +936,31 @@ class Cfft10:
     e2e_api = ("zldsp::fft::CFFT<float>(10).forward then .backward on host numpy buffers (the drop-in "
                "class, ZLFFT_MODE_HOST): one transform per call, synchronous, as the reference's callers make them")
 
+    def cpp_dropin_latency(self):
+        """The same pairs through the C++ drop-in class (tests/cpp/dropin_latency.cpp,
+        compiled here against include/ and libzlfft_cuda.so): the reference's
+        callers are C++, so this is their per-call cost without Python."""
+        import shutil
+        import subprocess
+        import tempfile
+        if shutil.which("g++") is None:
+            return {"error": "g++ not available"}
+        libdir = os.path.join(ROOT, "zldsp_fft_b200", "lib")
+        with tempfile.TemporaryDirectory() as td:
+            exe = os.path.join(td, "dropin_latency")
+            r = subprocess.run(["g++", "-std=c++20", "-O2", "-I", os.path.join(ROOT, "include"),
+                                os.path.join(ROOT, "tests", "cpp", "dropin_latency.cpp"), "-L", libdir,
+                                "-lzlfft_cuda", "-o", exe], capture_output=True, text=True)
+            if r.returncode != 0:
+                return {"error": r.stderr[-200:]}
+            env = dict(os.environ)
+            env["LD_LIBRARY_PATH"] = libdir + ":" + env.get("LD_LIBRARY_PATH", "")
+            r = subprocess.run([exe, str(self.order), "2000", "7"], capture_output=True, text=True, env=env,
+                               timeout=300)
+            if r.returncode != 0:
+                return {"error": (r.stdout + r.stderr)[-200:]}
+            return json.loads(r.stdout.strip().splitlines()[-1])
+
     def setup_e2e(self):
         n = 1 << self.order
         self.cf = self.Z.CFFT(self.order, np.float32)
@@ -1443,6 +1468,7 @@ def run_ours(args, wl_cls):
     pcie = pcie_probe()
     bound = e2e_bound(wl.bytes_per_step, wl.e2e_h2d, wl.e2e_d2h, pcie)
     schedules = wl.compare(stream, max(3, min(args.steps, 10))) if hasattr(wl, "compare") else None
+    cpp_latency = wl.cpp_dropin_latency() if (rank == 0 and hasattr(wl, "cpp_dropin_latency")) else None
 
     peak, peak_kind = measured_hbm_peak()
     dom = max(per_op_ms, key=per_op_ms.get)  # the op with the largest share of the step's time
@@ -1470,6 +1496,8 @@ def run_ours(args, wl_cls):
     }
     if schedules is not None:
         line["schedules"] = schedules
+    if cpp_latency is not None:
+        line["e2e"]["cpp_dropin"] = cpp_latency
     if rank == 0:
         if world == 1 and not args.no_cpu:
             try:
