@@ -543,7 +543,14 @@ cudaError_t launch_pre(const zlfft_plan_s* p, int in_layout, const void* i0, con
 zlfft::PassLaunchFn pick_pass(const zlfft_plan_s* p, int pi, bool fwd, int li, int lo) {
     const int P = p->cfft_order;
     if (p->tc_form && li == ZLFFT_AOS && lo == ZLFFT_AOS) {
-        zlfft::PassLaunchFn f = tables().tc.fn[P - zlfft::kPassMinP][pi][fwd ? 1 : 0];
+        // the pipelined kernel; ZLFFT_TC_PIPE=0 selects the serial one (comparison)
+        static const bool pipe = [] {
+            const char* e = getenv("ZLFFT_TC_PIPE");
+            return !(e && e[0] == '0');
+        }();
+        const auto& tt = tables().tc;
+        zlfft::PassLaunchFn f = pipe ? tt.pipe[P - zlfft::kPassMinP][pi][fwd ? 1 : 0] : nullptr;
+        if (!f) f = tt.fn[P - zlfft::kPassMinP][pi][fwd ? 1 : 0];
         if (f) return f;
     }
     const zlfft::PassTable& t = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;

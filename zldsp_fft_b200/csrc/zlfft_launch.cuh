@@ -15,6 +15,7 @@
 #include "zlfft_pass.cuh"
 #include "zlfft_resident.cuh"
 #include "zlfft_tc_pass.cuh"
+#include "zlfft_tc_pipe.cuh"
 #include "zlfft_tile.cuh"
 
 namespace zlfft {
@@ -294,6 +295,7 @@ void fill_pass_range(PassTable& t) {
 // passes of FP32 complex AoS data (null where a pass is not 256 points).
 struct TcPassTable {
     PassLaunchFn fn[kPassMaxP - kPassMinP + 1][kMaxPasses][2];
+    PassLaunchFn pipe[kPassMaxP - kPassMinP + 1][kMaxPasses][2];  // the pipelined kernel (zlfft_tc_pipe.cuh)
     int l_in[kPassMaxP - kPassMinP + 1][kMaxPasses];  // sub-length at the pass's entry
 };
 
@@ -341,14 +343,44 @@ cudaError_t launch_tc_pass(const PassArgs& a_in, cudaStream_t stream, const Laun
     return cudaGetLastError();
 }
 
+// The pipelined tensor-core pass: one CTA per SM, items streamed through it.
+template <int P, int PI, bool FWD>
+cudaError_t launch_tc_pipe(const PassArgs& a_in, cudaStream_t stream, const LaunchCtx& ctx) {
+    using Cfg = TcPipeCfg<P, PI>;
+    auto kern = tc_pipe_kernel<P, PI, FWD>;
+    PassArgs a = a_in;
+    PassMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    static const bool tma_enabled = [] {
+        const char* e = getenv("ZLFFT_PASS_TMA");
+        return !(e && e[0] == '0');
+    }();
+    a.tma = (tma_enabled && a.tma && !(Cfg::FIRST && a.gin0) && encode_pass_maps<float, P, PI, kAoS>(a, maps)) ? 1
+                                                                                                                 : 0;
+    static ResidentSlots slots;
+    (void)resident_ctas(slots, [kern] {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+        return 1;
+    });
+    if (a.batch <= 0) return cudaSuccess;
+    const long long items = a.batch * Cfg::CPT;
+    const unsigned grid = (unsigned)(items < ctx.num_sms ? items : ctx.num_sms);
+    kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(a, maps);
+    if (ctx.launches) ++*ctx.launches;
+    return cudaGetLastError();
+}
+
 template <int P, int PI>
 void fill_tc_pass_one(TcPassTable& t) {
     t.l_in[P - kPassMinP][PI] = PassCfg<float, P, PI>::L_IN;
     if constexpr (pass_radix(P, PI) == 256 && PassCfg<float, P, PI>::UPC == 16) {
         t.fn[P - kPassMinP][PI][1] = launch_tc_pass<P, PI, true>;
         t.fn[P - kPassMinP][PI][0] = launch_tc_pass<P, PI, false>;
+        t.pipe[P - kPassMinP][PI][1] = launch_tc_pipe<P, PI, true>;
+        t.pipe[P - kPassMinP][PI][0] = launch_tc_pipe<P, PI, false>;
     } else {
         t.fn[P - kPassMinP][PI][0] = t.fn[P - kPassMinP][PI][1] = nullptr;
+        t.pipe[P - kPassMinP][PI][0] = t.pipe[P - kPassMinP][PI][1] = nullptr;
     }
 }
 
