@@ -49,6 +49,8 @@ FORMS = {
     "fast": "fast-twiddle plain form: CUDA cores, radix-16 groups' twiddles from two table values per butterfly",
     "tc": "tensor-core split FP16 hi/lo, FP32 accumulate (256-point passes), plain elsewhere",
     "tuned": "autotuned per order among plain, fast-twiddle and tensor-core split forms (see schedules)",
+    "macro": "the reference's macro path (DIF macro stages + per-segment Stockham + transposed store) as a "
+             "small-cache host runs it, bit-identical to the reference there",
 }
 
 
@@ -400,7 +402,8 @@ class Cfft2G:
         self.form = form
         self.desc = self.desc + {"tc": ", tensor-core split FP16 hi/lo form", "fast": ", fast-twiddle form",
                                  "plain": ", plain form (the reference's arithmetic, bit-identical)",
-                                 "tuned": ", autotuned form per order"}[form]
+                                 "tuned": ", autotuned form per order",
+                                 "macro": ", the reference's macro DIF path (small-cache host switch)"}[form]
         self.op_bytes = {}
         for o in self.orders:
             for d in ("fwd", "bwd"):
@@ -411,13 +414,15 @@ class Cfft2G:
         import torch
         import zldsp_fft_b200 as Z
         self.Z = Z
-        mode = {"tc": Z.MODE_TC_FP16, "fast": Z.MODE_FAST, "plain": Z.MODE_PLAIN, "tuned": Z.MODE_TUNED}[self.form]
+        mode = {"tc": Z.MODE_TC_FP16, "fast": Z.MODE_FAST, "plain": Z.MODE_PLAIN, "tuned": Z.MODE_TUNED,
+                "macro": Z.MODE_PLAIN}[self.form]
         self.tuning = None
         if self.form == "tuned":  # set-up, outside the timed region
             for o in self.orders:
                 Z.autotune(Z.C2C, o, o, np.float32, device=device)
             self.tuning = {f"order{o}": Z.tuning(Z.C2C, o, np.float32, device=device) for o in self.orders}
-        self.plans = {o: Z.Plan(Z.C2C, o, np.float32, mode=mode, device=device) for o in self.orders}
+        sw = (10, 14) if self.form == "macro" else None
+        self.plans = {o: Z.Plan(Z.C2C, o, np.float32, mode=mode, device=device, switch=sw) for o in self.orders}
         g = torch.Generator(device=device)
         g.manual_seed(1003)
         # A: input (never overwritten), B: forward output, C: backward output
@@ -1520,9 +1525,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-autotune", action="store_true",
                     help="mixed only: skip the per-order autotuning in set-up (for profiling runs)")
-    ap.add_argument("--form", choices=["tuned", "plain", "fast", "tc"], default="tuned",
+    ap.add_argument("--form", choices=["tuned", "plain", "fast", "tc", "macro"], default="tuned",
                     help="cfft2g only: the autotuned form per order (default), the plain form (the reference's "
-                         "arithmetic), the fast-twiddle form, or the tensor-core split FP16 hi/lo form")
+                         "arithmetic), the fast-twiddle form, the tensor-core split FP16 hi/lo form, or the "
+                         "reference's macro DIF path as a small-cache host runs it")
     ap.add_argument("--total-log2", type=int, default=None,
                     help="cfft2g: complex elements per order = 2^k (default 28 = 2 GiB); stft / istft: signal "
                          "samples = 2^k (default 27); smaller cases are for profiling and are not the benchmark "

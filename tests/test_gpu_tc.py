@@ -138,3 +138,44 @@ def test_fast_twiddle_form_tile_orders(oracle, order):
         assert oracle.rel_l2(X, oracle.rfft_fp64(xr)).max() <= rtol
     Pw = G.run_r2c(rf, xr, sqr_mag=True)
     assert oracle.rel_l2(Pw, np.abs(oracle.rfft_fp64(xr)) ** 2).max() <= 2 * rtol
+
+
+def test_pipelined_tc_kernel_equals_serial_kernel():
+    """The warp-specialised pipelined tensor-core pass (ZLFFT_TC_PIPE=1, its own
+    process since the switch is read once) computes the serial kernel's
+    arithmetic in the same order: bit-identical outputs, orders 14, 16 and 20,
+    forward and backward, several chunks."""
+    import os
+    import subprocess
+    import sys
+    code = r'''
+import sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+import zldsp_fft_b200 as Z
+rng = np.random.default_rng(31)
+out = {}
+for order, b in ((14, 700), (16, 150), (20, 7)):
+    n = 1 << order
+    x = (rng.uniform(-1, 1, (b, n)) + 1j * rng.uniform(-1, 1, (b, n))).astype(np.complex64)
+    p = Z.Plan(Z.C2C, order, np.float32, Z.MODE_TC_FP16)
+    ti = torch.from_numpy(x.view(np.float32).reshape(b, n, 2).copy()).cuda()
+    f = torch.empty_like(ti); g = torch.empty_like(ti)
+    p.exec_device(Z.FORWARD, Z.AOS, Z.AOS, ti.data_ptr(), None, f.data_ptr(), None, b)
+    p.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, f.data_ptr(), None, g.data_ptr(), None, b)
+    torch.cuda.synchronize()
+    assert p.device_status() == 0
+    out[f"f{order}"] = f.cpu().numpy(); out[f"g{order}"] = g.cpu().numpy()
+np.savez(sys.argv[2], **out)
+'''
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = {}
+    for flag in ("0", "1"):
+        path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"zlfft_tcpipe_{flag}_{os.getpid()}.npz")
+        env = dict(os.environ, ZLFFT_TC_PIPE=flag)
+        r = subprocess.run([sys.executable, "-c", code, root, path], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        res[flag] = dict(np.load(path))
+        os.remove(path)
+    for k in res["0"]:
+        assert np.array_equal(res["0"][k], res["1"][k]), k

@@ -543,10 +543,12 @@ cudaError_t launch_pre(const zlfft_plan_s* p, int in_layout, const void* i0, con
 zlfft::PassLaunchFn pick_pass(const zlfft_plan_s* p, int pi, bool fwd, int li, int lo) {
     const int P = p->cfft_order;
     if (p->tc_form && li == ZLFFT_AOS && lo == ZLFFT_AOS) {
-        // the pipelined kernel; ZLFFT_TC_PIPE=0 selects the serial one (comparison)
+        // the serial kernel (tc_pass_kernel, three CTAs per SM); ZLFFT_TC_PIPE=1 selects the
+        // warp-specialised pipelined one (tc_pipe_kernel), measured slower on B200: its phases
+        // get 4 warps each where the serial kernel runs 24 warps per SM through every phase
         static const bool pipe = [] {
             const char* e = getenv("ZLFFT_TC_PIPE");
-            return !(e && e[0] == '0');
+            return e && e[0] == '1';
         }();
         const auto& tt = tables().tc;
         zlfft::PassLaunchFn f = pipe ? tt.pipe[P - zlfft::kPassMinP][pi][fwd ? 1 : 0] : nullptr;
