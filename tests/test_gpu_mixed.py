@@ -232,3 +232,27 @@ def test_exec_mixed_device_one_shot(oracle):
         assert np.array_equal(y, _oracle(oracle, s, x)), s
     # an empty batch is a no-op
     assert Z._capi.lib().zlfft_exec_mixed_device(None, 0, None) == 0
+
+
+def test_mixed_orders_6_to_20_all_schedules(oracle):
+    """A batch over the whole range of the mixed-order target, 2^6 to 2^20,
+    CFFT forward/backward and RFFT forward/forward_sqr_mag/backward, FP32:
+    both persistent classes (complex orders 2..11 and 12..13), the order-14
+    tile and the multi-pass pipelines (up to 2^20, several transforms per
+    order). Every schedule gives the oracle's bits for every transform."""
+    rng = np.random.default_rng(2020)
+    specs = []
+    for order in range(6, 21):
+        reps = 6 if order <= 13 else (3 if order <= 17 else 2)
+        for _ in range(reps):
+            specs.append((Z.C2C, order, Z.FORWARD, Z.F32))
+            specs.append((Z.C2C, order, Z.BACKWARD, Z.F32))
+            specs.append((Z.R2C, order, (Z.FORWARD, Z.FORWARD_SQR_MAG, Z.BACKWARD)[int(rng.integers(3))], Z.F32))
+    order_perm = rng.permutation(len(specs))
+    specs = [specs[i] for i in order_perm]
+    pk = Packed(rng, specs)
+    expect = [_oracle(oracle, s, x) for s, x in zip(specs, pk.x)]
+    for sched in (Z.SCHED_PER_ORDER, Z.SCHED_PERSISTENT, Z.SCHED_GRAPH):
+        _, res = _run(pk, sched)
+        bad = [i for i, (y, e) in enumerate(zip(res, expect)) if not np.array_equal(y, e)]
+        assert not bad, (sched, [specs[i] for i in bad[:5]], len(bad))

@@ -1472,9 +1472,10 @@ int exec_host_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const
 // A mixed batch is sorted on the host into groups of one (precision, kind,
 // order, operation); each group's transforms are addressed through gathered
 // pointer arrays (transform t of the group reads gin[t], writes gout[t]).
-// Groups whose complex order fits a 128-thread tile (2..11) become tiles of
-// one persistent launch per precision (zlfft_mixed.cuh); the others run as
-// gathered batched launches of the tile kernel (orders 0, 1, 12, 13) or of
+// Groups of complex order 2..13 become tiles of persistent launches, one per
+// (precision, order class): orders 2..11 in 128-thread CTAs, 12..13 in
+// 512-thread CTAs (zlfft_mixed.cuh); the others run as gathered batched
+// launches of the tile kernel (orders 0, 1 and the FP32 order-14 tile) or of
 // the multi-pass pipeline (14 and up), largest first.
 struct MixedGroupHost {
     zlfft_plan plan;
@@ -1496,9 +1497,9 @@ struct zlfft_mixed_s {
     const void** d_gin = nullptr;
     void** d_gout = nullptr;
     zlfft::MixedGroup* d_mgroups[2] = {nullptr, nullptr};  // per precision
-    zlfft::MixedItem* d_items[2] = {nullptr, nullptr};
-    int n_items[2] = {0, 0};
-    int* d_counter = nullptr;  // one work-list counter per precision
+    zlfft::MixedItem* d_items[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [precision][order class]
+    int n_items[2][2] = {{0, 0}, {0, 0}};
+    int* d_counter = nullptr;  // one work-list counter per (precision, order class)
     cudaStream_t cap_stream = nullptr;
     // persistent schedule: the multi-pass and large-tile groups run on these
     // streams (forked from the caller's stream, joined back) beside the
@@ -1621,7 +1622,7 @@ zlfft::TileArgs mixed_args(const zlfft_mixed_s* m, const MixedGroupHost& g) {
     return a;
 }
 
-bool mixed_in_persistent(const MixedGroupHost& g) { return g.P >= zlfft::kMixedMinP && g.P <= zlfft::kMixedMaxP; }
+bool mixed_in_persistent(const MixedGroupHost& g) { return g.P >= zlfft::kMixedMinP && g.P <= zlfft::kMixedTopP; }
 
 // One group as its own batched launch(es) on `st`.
 int mixed_run_group(zlfft_mixed_s* m, const MixedGroupHost& g, cudaStream_t st) {
@@ -1668,15 +1669,19 @@ int mixed_run(zlfft_mixed_s* m, int schedule, cudaStream_t st) {
             if (rc) return rc;
         }
     }
-    for (int pr = 0; pr < 2; ++pr) {
-        if (!m->n_items[pr]) continue;
-        ZL_CUDA(cudaMemsetAsync(m->d_counter + pr, 0, sizeof(int), st));
-        cudaError_t e = pr == 0 ? zlfft::launch_mixed_f32(m->d_mgroups[0], m->d_items[0], m->n_items[0],
-                                                          m->d_counter, st, m->num_sms)
-                                : zlfft::launch_mixed_f64(m->d_mgroups[1], m->d_items[1], m->n_items[1],
-                                                          m->d_counter + 1, st, m->num_sms);
-        if (e != cudaSuccess) return cuda_fail(e, "persistent mixed launch");
-        ++m->launches;
+    // the 512-thread class first: its tiles are the longest
+    for (int cls = 1; cls >= 0; --cls) {
+        for (int pr = 0; pr < 2; ++pr) {
+            if (!m->n_items[pr][cls]) continue;
+            int* ctr = m->d_counter + 2 * pr + cls;
+            ZL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(int), st));
+            cudaError_t e = pr == 0 ? zlfft::launch_mixed_f32(cls, m->d_mgroups[0], m->d_items[0][cls],
+                                                              m->n_items[0][cls], ctr, st, m->num_sms)
+                                    : zlfft::launch_mixed_f64(cls, m->d_mgroups[1], m->d_items[1][cls],
+                                                              m->n_items[1][cls], ctr, st, m->num_sms);
+            if (e != cudaSuccess) return cuda_fail(e, "persistent mixed launch");
+            ++m->launches;
+        }
     }
     if (big) {
         for (int i = 0; i < zlfft_mixed_s::kSideStreams; ++i) {
@@ -1754,48 +1759,55 @@ int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int d
     }
     // device block: gather arrays, then per precision the group records and work lists
     std::vector<zlfft::MixedGroup> mg[2];
-    std::vector<zlfft::MixedItem> items[2];
-    std::vector<long long> cost[2];
+    std::vector<zlfft::MixedItem> items[2][2];  // [precision][order class]
+    std::vector<long long> cost[2][2];
     const size_t gin_off = 0, gout_off = n * sizeof(void*);
     size_t off = 2 * n * sizeof(void*);
     auto align_up = [](size_t v) { return (v + 255) & ~size_t{255}; };
     for (const MixedGroupHost& g : m->groups) {
         if (!mixed_in_persistent(g)) continue;
         const int pr = g.prec == ZLFFT_F32 ? 0 : 1;
+        const int cls = zlfft::mixed_class(g.P);
         const int tpc = zlfft::mixed_tpc(g.P);
         const long long tiles = ((long long)g.count + tpc - 1) / tpc;
         for (long long t = 0; t < tiles; ++t) {
-            items[pr].push_back(zlfft::MixedItem{(int)mg[pr].size(), (int)t});
-            cost[pr].push_back(mixed_tile_cost(g.P));
+            items[pr][cls].push_back(zlfft::MixedItem{(int)mg[pr].size(), (int)t});
+            cost[pr][cls].push_back(mixed_tile_cost(g.P));
         }
         mg[pr].push_back(zlfft::MixedGroup{zlfft::TileArgs{}, zlfft::mixed_code(g.dop, g.P)});
     }
     for (int pr = 0; pr < 2; ++pr) {
-        // longest tiles first (groups are already in descending order; keep it stable)
-        std::vector<size_t> o(items[pr].size());
-        for (size_t i = 0; i < o.size(); ++i) o[i] = i;
-        std::stable_sort(o.begin(), o.end(), [&](size_t x, size_t y) { return cost[pr][x] > cost[pr][y]; });
-        std::vector<zlfft::MixedItem> sorted(o.size());
-        for (size_t i = 0; i < o.size(); ++i) sorted[i] = items[pr][o[i]];
-        items[pr].swap(sorted);
-        if (items[pr].size() > (size_t)INT32_MAX) {
-            mixed_release(m);
-            return fail(ZLFFT_ERR_INVALID_ARG, "too many tiles");
+        for (int cls = 0; cls < 2; ++cls) {
+            // longest tiles first (groups are already in descending order; keep it stable)
+            std::vector<zlfft::MixedItem>& it = items[pr][cls];
+            std::vector<size_t> o(it.size());
+            for (size_t i = 0; i < o.size(); ++i) o[i] = i;
+            std::stable_sort(o.begin(), o.end(),
+                             [&](size_t x, size_t y) { return cost[pr][cls][x] > cost[pr][cls][y]; });
+            std::vector<zlfft::MixedItem> sorted(o.size());
+            for (size_t i = 0; i < o.size(); ++i) sorted[i] = it[o[i]];
+            it.swap(sorted);
+            if (it.size() > (size_t)INT32_MAX) {
+                mixed_release(m);
+                return fail(ZLFFT_ERR_INVALID_ARG, "too many tiles");
+            }
+            m->n_items[pr][cls] = (int)it.size();
         }
-        m->n_items[pr] = (int)items[pr].size();
     }
-    size_t grp_off[2], item_off[2];
+    size_t grp_off[2], item_off[2][2];
     for (int pr = 0; pr < 2; ++pr) {
         off = align_up(off);
         grp_off[pr] = off;
         off += mg[pr].size() * sizeof(zlfft::MixedGroup);
-        off = align_up(off);
-        item_off[pr] = off;
-        off += items[pr].size() * sizeof(zlfft::MixedItem);
+        for (int cls = 0; cls < 2; ++cls) {
+            off = align_up(off);
+            item_off[pr][cls] = off;
+            off += items[pr][cls].size() * sizeof(zlfft::MixedItem);
+        }
     }
     off = align_up(off);
     const size_t counter_off = off;
-    off += 2 * sizeof(int);
+    off += 4 * sizeof(int);
     if (cudaMalloc(&m->d_mem, off) != cudaSuccess) {
         cudaGetLastError();
         mixed_release(m);
@@ -1821,15 +1833,17 @@ int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int d
     }
     for (int pr = 0; pr < 2 && e == cudaSuccess; ++pr) {
         m->d_mgroups[pr] = reinterpret_cast<zlfft::MixedGroup*>(base + grp_off[pr]);
-        m->d_items[pr] = reinterpret_cast<zlfft::MixedItem*>(base + item_off[pr]);
         if (!mg[pr].empty())
             e = cudaMemcpy(m->d_mgroups[pr], mg[pr].data(), mg[pr].size() * sizeof(zlfft::MixedGroup),
                            cudaMemcpyHostToDevice);
-        if (e == cudaSuccess && !items[pr].empty())
-            e = cudaMemcpy(m->d_items[pr], items[pr].data(), items[pr].size() * sizeof(zlfft::MixedItem),
-                           cudaMemcpyHostToDevice);
+        for (int cls = 0; cls < 2 && e == cudaSuccess; ++cls) {
+            m->d_items[pr][cls] = reinterpret_cast<zlfft::MixedItem*>(base + item_off[pr][cls]);
+            if (!items[pr][cls].empty())
+                e = cudaMemcpy(m->d_items[pr][cls], items[pr][cls].data(),
+                               items[pr][cls].size() * sizeof(zlfft::MixedItem), cudaMemcpyHostToDevice);
+        }
     }
-    if (e == cudaSuccess) e = cudaMemset(m->d_counter, 0, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(m->d_counter, 0, 4 * sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&m->cap_stream, cudaStreamNonBlocking);
     for (int i = 0; i < zlfft_mixed_s::kSideStreams && e == cudaSuccess; ++i) {
         e = cudaStreamCreateWithFlags(&m->side[i], cudaStreamNonBlocking);

@@ -1,9 +1,9 @@
-// Instantiates the persistent mixed-order kernel in float.
+// Instantiates the persistent mixed-order kernels (both order classes) in float.
 #include "zlfft_mixed.cuh"
 
 namespace zlfft {
-cudaError_t launch_mixed_f32(const MixedGroup* groups, const MixedItem* items, int n_items, int* counter,
+cudaError_t launch_mixed_f32(int cls, const MixedGroup* groups, const MixedItem* items, int n_items, int* counter,
                              cudaStream_t stream, int num_sms) {
-    return launch_mixed<float>(groups, items, n_items, counter, stream, num_sms);
+    return launch_mixed<float>(cls, groups, items, n_items, counter, stream, num_sms);
 }
 }  // namespace zlfft
