@@ -538,6 +538,16 @@ cudaError_t launch_pre(const zlfft_plan_s* p, int in_layout, const void* i0, con
     return cudaGetLastError();
 }
 
+// Intermediates between passes are dropped from L2 once read (pass_kernel,
+// discard_in); ZLFFT_L2_DISCARD=0 keeps them (comparison).
+bool l2_discard_enabled() {
+    static const bool on = [] {
+        const char* e = getenv("ZLFFT_L2_DISCARD");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 // Kernel of pass pi: the tensor-core split-precision pass where the plan asks
 // for it and one exists (256-point passes, FP32 AoS), else the plain pass.
 zlfft::PassLaunchFn pick_pass(const zlfft_plan_s* p, int pi, bool fwd, int li, int lo) {
@@ -648,6 +658,7 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
             pa.tctw = p->d_tctw ? static_cast<const char*>(p->d_tctw) + p->tctw_off[pi] * 2 * p->esize : nullptr;
             pa.err = p->d_err;
             pa.tma_out = (p->store_tma < 0 ? p->prec == ZLFFT_F32 : p->store_tma == 1) ? 1 : 0;
+            pa.discard_in = (l2_discard_enabled() && (pi > 0 || c2r)) ? 1 : 0;  // the input is dead scratch
             if (gfirst) {
                 pa.gin0 = gi0;
                 pa.gin1 = gi1;
@@ -1185,6 +1196,7 @@ int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layo
             pa.tctw = p->d_tctw ? static_cast<const char*>(p->d_tctw) + p->tctw_off[pi] * 2 * p->esize : nullptr;
             pa.err = p->d_err;
             pa.tma_out = (p->store_tma < 0 ? p->prec == ZLFFT_F32 : p->store_tma == 1) ? 1 : 0;
+            pa.discard_in = (l2_discard_enabled() && (pi > 0 || c2r)) ? 1 : 0;  // the input is dead scratch
             const size_t eb = (pi == 0 && src_layout == ZLFFT_SOA) ? p->esize : cx;
             pa.tma = (p->use_tma && aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
                       (nb == 1 || ((size_t)src_stride * eb) % 16 == 0)) ? 1 : 0;

@@ -245,6 +245,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     return false;
 }
 
+// Drops one 128-byte line of global memory from L2 without writing it back
+// (its contents become undefined): for intermediates that no later kernel
+// reads, so that the dead data does not cost DRAM write bandwidth when L2
+// evicts it. The address must be 128-byte aligned.
+__device__ __forceinline__ void discard_l2_line(const void* p) {
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
 // Device error word bits (read back by the host with zlfft_plan_device_status).
 constexpr int kDevErrWaitTimeout = 1;
 

@@ -124,6 +124,7 @@ struct PassArgs {
     int tma_out;           // first pass: the output map (PassMaps::mo) is valid, store by TMA
     int* err;              // device error word (kDevErrWaitTimeout on a timed-out wait)
     int tma;               // the tensor maps describe the input (else direct loads)
+    int discard_in;        // the input is scratch that nothing reads after this pass: drop it from L2
     // Gathered transforms (mixed batches): the first pass reads transform t
     // at gin0[t] (gin1[t]) and the last pass writes it at gout0[t] (gout1[t]).
     const void* const* gin0;
@@ -424,6 +425,24 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                 }(),
                 ...);
         }(std::make_integer_sequence<int, GE - GB>{});
+        // The item's input rows (UPC consecutive units x R positions of AoS
+        // scratch: each position's units are one run of UPC * sizeof(C) bytes)
+        // are dead when nothing reads them after this pass: drop them from L2
+        // rather than let L2 write them back to DRAM. Every thread's loaded
+        // values have fed its stores of this item, so after the barrier no load
+        // of the item is outstanding.
+        if constexpr (IL2 == kAoS && SPLIT == 0 && (UPC * sizeof(C)) % 128 == 0) {
+            if (a.discard_in) {
+                __syncthreads();
+                constexpr int LPR = (int)(UPC * sizeof(C)) / 128;  // lines per position row
+                const char* ib =
+                    reinterpret_cast<const char*>(static_cast<const C*>(a.in0) + tr * a.in_stride + (U - u));
+                for (int l = (int)threadIdx.x; l < R * LPR; l += Cfg::THREADS) {
+                    const int pos = l / LPR, sub = l % LPR;
+                    discard_l2_line(ib + (size_t)pos * (N / R) * sizeof(C) + (size_t)sub * 128);
+                }
+            }
+        }
         if constexpr (SPLIT != 0) {
             // ---- fused RFFT split over the item's mirror pairs (M = N complex points)
             __syncthreads();
