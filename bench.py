@@ -1364,6 +1364,71 @@ def config_of(wl, world):
             "parallelism": f"replicas x{world}"}
 
 
+# ------------------------------------------------------------------ the other configurations
+OTHER_CONFIGS = (("rfft12", "cfg 2"), ("mixed", "cfg 4"), ("cfft64", "cfg 5"), ("cfft10", "cfg 1"))
+
+
+def quick_measure(wl, device, steps=5, warmup=3):
+    """One configuration measured the way the main line is (rotating sets or
+    L2 flush as the workload defines, CUDA events on the launching stream,
+    clocks sampled), with fewer steps and without the host-API and CPU legs:
+    the evidence for the benchmark configurations other than the default."""
+    import torch
+    wl.setup(device)
+    stream = torch.cuda.current_stream()
+    st = stream.cuda_stream
+    for w in range(warmup):
+        for _, fn in wl.ops(w):
+            fn(st)
+    torch.cuda.synchronize()
+    wl.take_launches()
+    names = [name for name, _ in wl.ops(0)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)] for _ in range(steps)]
+    flush = getattr(wl, "flush", None)
+    clocks = ClockSampler(device)
+    clocks.start()
+    for s in range(steps):
+        if flush is not None:
+            flush(st)
+        ops = wl.ops(s)
+        ev[s][0].record(stream)
+        for i, (_, fn) in enumerate(ops):
+            fn(st)
+            ev[s][i + 1].record(stream)
+    torch.cuda.synchronize()
+    clocks.stop()
+    launches = wl.take_launches()
+    elapsed_ms = sum(ev[s][0].elapsed_time(ev[s][-1]) for s in range(steps))
+    per_op_ms = {name: statistics.mean(ev[s][i].elapsed_time(ev[s][i + 1]) for s in range(steps))
+                 for i, name in enumerate(names)}
+    peak, peak_kind = measured_hbm_peak()
+    dom = max(per_op_ms, key=per_op_ms.get)
+    achieved = wl.op_bytes[dom] / (per_op_ms[dom] / 1e3) / 1e9
+    res = {"workload": wl.desc, "dtype": wl.dtype, "steps": steps, "warmup": warmup,
+           "value": round(wl.bytes_per_step * steps / (elapsed_ms / 1e3) / 1e9, 2), "unit": "GB/s",
+           "ms_per_step": round(elapsed_ms / steps, 4),
+           "roofline": {"kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                        "frac": round(achieved / peak, 4), "peak_source": peak_kind},
+           "per_op_gbs": {k: round(wl.op_bytes[k] / (v / 1e3) / 1e9, 1) for k, v in per_op_ms.items()},
+           "per_op_us": {k: round(v * 1e3, 2) for k, v in per_op_ms.items()},
+           "gpu_launches": launches, "clocks": clocks.summary()}
+    if hasattr(wl, "compare"):
+        res["schedules"] = wl.compare(stream, 3)
+    return res
+
+
+def measure_other_configs(device):
+    out = {}
+    for name, label in OTHER_CONFIGS:
+        try:
+            r = quick_measure(WORKLOADS[name](), device)
+            r["config"] = label
+            out[name] = r
+        except Exception as e:  # reported, never required: the main line stands on its own
+            out[name] = {"config": label, "error": str(e)[:200]}
+    return out
+
+
 # ------------------------------------------------------------------ arms
 def run_reference_arm(args, wl_cls):
     rank = int(os.environ.get("RANK", "0"))
@@ -1503,6 +1568,8 @@ def run_ours(args, wl_cls):
         line["schedules"] = schedules
     if cpp_latency is not None:
         line["e2e"]["cpp_dropin"] = cpp_latency
+    if rank == 0 and world == 1 and args.workload == "cfft2g" and not args.no_configs:
+        line["other_configs"] = measure_other_configs(device)
     if rank == 0:
         if world == 1 and not args.no_cpu:
             try:
@@ -1523,6 +1590,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cfft2g")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="default workload only: skip the short measurement of the other benchmark configurations "
+                         "(other_configs in the line)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="mixed only: skip the per-order autotuning in set-up (for profiling runs)")
     ap.add_argument("--form", choices=["tuned", "plain", "fast", "tc", "macro"], default="tuned",
