@@ -234,3 +234,34 @@ def test_host_mode_follows_this_hosts_switch(oracle):
                 x = _cx(np.random.default_rng(order), 1, 1 << order, ct)
                 with oracle.hybrid(prec, l1, sw):
                     assert np.array_equal(run_c2c(p, x, True), oracle.cfft_port(x, True)), order
+
+
+def test_macro_cfft_f32_orders_24_and_26(oracle):
+    """The largest macro orders (seven and eight DIF stages in two passes,
+    micro order 10): order 24 forward bit-identical to the restatement; order
+    26 (512 MiB per transform) round trip and Parseval within the FP32 bar,
+    computed on the device."""
+    import torch
+    rng = np.random.default_rng(4600)
+    x = _cx(rng, 1, 1 << 24, np.complex64)
+    plan = Z.Plan(Z.C2C, 24, np.float32, switch=HOST["f32"])
+    assert plan.micro_order() == 10
+    with oracle.macro_host("f32"):
+        assert np.array_equal(run_c2c(plan, x, True), oracle.cfft_port(x, True))
+    del x
+    n = 1 << 26
+    plan = Z.Plan(Z.C2C, 26, np.float32, switch=HOST["f32"])
+    g = torch.Generator(device="cuda")
+    g.manual_seed(4601)
+    a = (torch.rand((n, 2), generator=g, device="cuda") * 2 - 1).contiguous()
+    y = torch.empty_like(a)
+    z = torch.empty_like(a)
+    plan.exec_device(Z.FORWARD, Z.AOS, Z.AOS, a.data_ptr(), None, y.data_ptr(), None, 1)
+    plan.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, y.data_ptr(), None, z.data_ptr(), None, 1)
+    torch.cuda.synchronize()
+    assert plan.device_status() == 0
+    xd, yd, zd = (torch.view_as_complex(t.double()) for t in (a, y, z))
+    bar = oracle.tolerance(26, "f32")
+    nx = torch.linalg.vector_norm(xd)
+    assert (torch.linalg.vector_norm(zd - n * xd) / (n * nx)).item() <= 2 * bar
+    assert abs((torch.linalg.vector_norm(yd) ** 2 - n * nx ** 2).item()) / (n * nx.item() ** 2) <= 4 * bar
