@@ -252,10 +252,11 @@ def test_bounded_wait_reports_instead_of_hanging():
 
 
 @pytest.mark.parametrize("prec,ft,ct", PRECS)
-@pytest.mark.parametrize("order", [14, 15, 16, 17, 18, 19, 20])
+@pytest.mark.parametrize("order", [14, 15, 16, 17, 18, 19, 20, 23])
 def test_multipass_cfft(oracle, prec, ft, ct, order):
     """Orders above one CTA: 2-3 Stockham passes through L2-resident scratch;
-    the arithmetic is still the reference's, so f32 stays bit-exact."""
+    the arithmetic is still the reference's, so f32 stays bit-exact. Orders 17,
+    18 and 23 start with a 512- or 1024-point pass (64- / 32-byte unit rows)."""
     n = 1 << order
     rng = np.random.default_rng(3000 + order)
     b = 2
@@ -274,7 +275,7 @@ def test_multipass_cfft(oracle, prec, ft, ct, order):
 
 
 @pytest.mark.parametrize("prec,ft,ct", PRECS)
-@pytest.mark.parametrize("order", [15, 16, 17])
+@pytest.mark.parametrize("order", [15, 16, 17, 18, 19])
 def test_multipass_rfft(oracle, prec, ft, ct, order):
     n = 1 << order
     rng = np.random.default_rng(4000 + order)

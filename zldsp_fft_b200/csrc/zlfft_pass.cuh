@@ -77,7 +77,15 @@ struct PassCfg {
     }();
     static constexpr int T = R / E;  // threads per unit
     static constexpr int UMIN = 128 / (int)sizeof(C);  // units per 128-byte row
-    static constexpr int UPC = (128 * E / R) > UMIN ? (128 * E / R) : UMIN;  // units per CTA
+    // Units per CTA: whole 128-byte rows up to 256-point passes (256 threads);
+    // the 512- and 1024-point passes keep 256 threads with 64- / 32-byte rows
+    // (FP32), which leaves room for TMA staging and 2-3 resident CTAs. Measured
+    // against 128-byte rows (CFFT<float> fast form, GB/s): order 17 (a 512-point
+    // pass) 2571 -> 2942; order 18 (a 1024-point pass) 2117 -> 2670; FP64
+    // order 18 2059 -> 2407.
+    // (The passes below 256 points keep 128 threads: 256 measured 2-16% slower
+    // at orders 19-21.)
+    static constexpr int UPC = R >= 512 ? 256 * E / R : ((128 * E / R) > UMIN ? (128 * E / R) : UMIN);
     static constexpr int ROW = UPC + 1;
     static constexpr int THREADS = UPC * T;
     static constexpr size_t XBYTES = (size_t)R * ROW * sizeof(C);  // exchange buffer (padded rows)
