@@ -15,7 +15,9 @@
 // ROW = UPC + 1. Lanes run over units fastest, so every read, exchange write
 // and global access of a half-warp touches 16 consecutive units (128 bytes
 // of f32 complex) of one position, and the padded row also makes the
-// column-wise copy-out of the first pass conflict-free.
+// column-wise copy-out of the first pass conflict-free. The 512- and
+// 1024-point passes have fewer units per CTA; their rows share 128-byte lines
+// and use an XOR-swizzled layout (pass_xidx).
 //
 // The first pass (sub-length 1 -> R) writes each unit's R results
 // contiguously, so its CTA output is one contiguous block, copied out of
@@ -88,7 +90,12 @@ struct PassCfg {
     static constexpr int UPC = R >= 512 ? 256 * E / R : ((128 * E / R) > UMIN ? (128 * E / R) : UMIN);
     static constexpr int ROW = UPC + 1;
     static constexpr int THREADS = UPC * T;
-    static constexpr size_t XBYTES = (size_t)R * ROW * sizeof(C);  // exchange buffer (padded rows)
+    // Exchange layout. Rows of 128 bytes or more: [pos][unit] with one padding
+    // element per row. Shorter rows (KROWS position rows per 128-byte line) are
+    // unpadded and XOR-swizzled instead (pass_xidx).
+    static constexpr int SLOTS = 128 / (int)sizeof(C);  // elements per 128-byte line
+    static constexpr int KROWS = UPC >= SLOTS ? 1 : SLOTS / UPC;
+    static constexpr size_t XBYTES = (size_t)R * (KROWS > 1 ? UPC : ROW) * sizeof(C);  // exchange buffer
     static constexpr size_t SOFF = (XBYTES + 127) / 128 * 128;     // staging offset (128-byte aligned)
     static constexpr size_t SBYTES = (size_t)R * UPC * sizeof(C);  // staging buffer
     // The next item's input (a box of UPC units x R positions) is prefetched
@@ -150,6 +157,50 @@ struct PassMaps {
     CUtensorMap mo;  // first pass: the output, as rows of R points (one row per unit)
 };
 
+// XOR of the base-K digits of x (K = 2 or 4, x < 2^16). Linear over bits:
+// the fold of a | b (disjoint bits) is fold(a) ^ fold(b).
+template <int K>
+__host__ __device__ constexpr int digit_fold(int x) {
+    static_assert(K == 2 || K == 4, "two or four position rows per line");
+    if constexpr (K == 4) {
+        x ^= x >> 2;
+        x ^= x >> 4;
+        x ^= x >> 8;
+        return x & 3;
+    } else {
+        x ^= x >> 1;
+        x ^= x >> 2;
+        x ^= x >> 4;
+        x ^= x >> 8;
+        return x & 1;
+    }
+}
+
+// Exchange-buffer index of position pt | pc (disjoint bits: pt the thread's
+// part, pc a part the compiler knows) and unit slot u.
+// - 128-byte rows or more (KROWS == 1): [pos][u] with rows of UPC + 1.
+// - Shorter rows: K = KROWS rows share a 128-byte line (line = pos / K). Row
+//   pos takes row slot fold_K(pos) of its line, the XOR of pos's base-K
+//   digits, and unit u takes slot u ^ (line mod UPC). The lanes of a half-warp
+//   (a quarter-warp in FP64) then touch distinct banks for every access of the
+//   kernel: K consecutive positions (group reads, position-major writes),
+//   positions 2^j apart (a radix group's writes at sub-length ELL), and one
+//   unit's consecutive positions (the first pass's copy-out). The padded
+//   layout puts positions 16 apart on one bank; measured on the 1024-point
+//   pass of CFFT<float> order 18, 40% of its shared-memory wavefronts were
+//   conflicts.
+template <class Cfg>
+__device__ __forceinline__ int pass_xidx(int pt, int pc, int u) {
+    if constexpr (Cfg::KROWS == 1) {
+        return (pt + pc) * Cfg::ROW + u;
+    } else {
+        constexpr int K = Cfg::KROWS, LK = K == 4 ? 2 : 1;
+        const int lt = pt >> LK, lc = pc >> LK;
+        const int x = ((digit_fold<K>(pt) ^ digit_fold<K>(pc)) * Cfg::UPC) | ((u ^ lt ^ lc) & (Cfg::UPC - 1));
+        return (lt + lc) * Cfg::SLOTS + x;
+    }
+}
+
 // Unit of slot u in work item ib of a last pass with the RFFT split fused:
 // the first half of the slots take units HALF*ib + u, the second half their
 // mirrors L_in - (HALF*ib + u) (unit L_in/2 stands in for the mirror of unit
@@ -202,7 +253,8 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
     C* stage = reinterpret_cast<C*>(smem + Cfg::SOFF);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + Cfg::SOFF + Cfg::SBYTES);
     const bool store_tma = Cfg::kStoreTMA && a.tma_out;
-    static_assert(SPLIT == 0 || (Cfg::LAST && FWD && L_IN > 1 && Cfg::UPC >= 2), "split fusion: RFFT forward last pass");
+    static_assert(SPLIT == 0 || (Cfg::LAST && FWD && L_IN > 1 && Cfg::UPC >= 2 && Cfg::KROWS == 1),
+                  "split fusion: RFFT forward last pass (padded layout)");
     const bool use_tma = Cfg::kTMA && a.tma && SPLIT == 0;
     auto issue = [&](long long it) {  // one thread issues the item's box copies
         if (!use_tma || threadIdx.x != 0 || it >= items) return;
@@ -324,7 +376,8 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                         for (int i = 0; i < NB; ++i) {
                             const int b = tb + i * T;
 #pragma unroll
-                            for (int rho = 0; rho < G.R; ++rho) v[i * G.R + rho] = sm[(b + rho * (R / G.R)) * ROW + u];
+                            for (int rho = 0; rho < G.R; ++rho)
+                                v[i * G.R + rho] = sm[pass_xidx<Cfg>(tb, b - tb + rho * (R / G.R), u)];
                         }
                     }
                     // ---- compute (global twiddles: kk = ku + L_IN * k_local)
@@ -343,11 +396,13 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                         __syncthreads();
 #pragma unroll
                         for (int i = 0; i < NB; ++i) {
-                            const int b = tb + i * T;
-                            const int Jl = b / ELL, kl = b % ELL;
+                            // position Jl * R_g * ELL + kl + mu * ELL of butterfly b = tb + i * T
+                            // (Jl = b / ELL, kl = b % ELL), split into the parts of tb and i * T
+                            const int pt = (tb / ELL) * G.R * ELL + tb % ELL;
+                            const int pi = ((i * T) / ELL) * G.R * ELL + (i * T) % ELL;
 #pragma unroll
                             for (int s = 0; s < G.R; ++s)
-                                sm[(Jl * G.R * ELL + kl + group_mu(G, s) * ELL) * ROW + u] = v[i * G.R + s];
+                                sm[pass_xidx<Cfg>(pt, pi + group_mu(G, s) * ELL, u)] = v[i * G.R + s];
                         }
                         __syncthreads();
                     } else if constexpr (L_IN == 1) {
@@ -393,17 +448,31 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                         for (int i = 0; i < NB; ++i) {
                             const int b = tb + i * T;  // J_local == 0 in the last group
 #pragma unroll
-                            for (int s = 0; s < G.R; ++s) sm[(b + group_mu(G, s) * ELL) * ROW + u] = v[i * G.R + s];
+                            for (int s = 0; s < G.R; ++s)
+                                sm[pass_xidx<Cfg>(tb, b - tb + group_mu(G, s) * ELL, u)] = v[i * G.R + s];
                         }
                         __syncthreads();
                         const bool g = Cfg::LAST && a.gout0 != nullptr;
                         const CxOut<F, OL2> out(g ? a.gout0[tr] : a.out0, g ? (a.gout1 ? a.gout1[tr] : nullptr) : a.out1,
                                                 (g ? 0 : tr * a.out_stride) + (long long)(U - u) * R);
+                        if constexpr (Cfg::KROWS == 1) {
 #pragma unroll 4
-                        for (int e = (int)threadIdx.x; e < UPC * R; e += Cfg::THREADS) {
-                            const int uu = e / R, pos = e % R;
-                            const C x = sm[pos * ROW + uu];
-                            out.put(e, (Cfg::LAST && !FWD) ? cswap(x) : x);
+                            for (int e = (int)threadIdx.x; e < UPC * R; e += Cfg::THREADS) {
+                                const int uu = e / R, pos = e % R;
+                                const C x = sm[pos * ROW + uu];
+                                out.put(e, (Cfg::LAST && !FWD) ? cswap(x) : x);
+                            }
+                        } else {
+                            // element e = t + k * THREADS: unit e / R = k * THREADS / R, position
+                            // t + (k * THREADS) % R (THREADS divides R here)
+                            static_assert(R % Cfg::THREADS == 0, "swizzled copy-out: whole passes over R");
+                            const int t = (int)threadIdx.x;
+#pragma unroll
+                            for (int k = 0; k < UPC * R / Cfg::THREADS; ++k) {
+                                const int e = t + k * Cfg::THREADS;
+                                const C x = sm[pass_xidx<Cfg>(t, (k * Cfg::THREADS) % R, (k * Cfg::THREADS) / R)];
+                                out.put(e, (Cfg::LAST && !FWD) ? cswap(x) : x);
+                            }
                         }
                         __syncthreads();
                     } else if constexpr (SPLIT != 0) {
@@ -413,7 +482,8 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
                         for (int i = 0; i < NB; ++i) {
                             const int b = tb + i * T;
 #pragma unroll
-                            for (int s = 0; s < G.R; ++s) sm[(b + group_mu(G, s) * ELL) * ROW + u] = v[i * G.R + s];
+                            for (int s = 0; s < G.R; ++s)
+                                sm[pass_xidx<Cfg>(tb, b - tb + group_mu(G, s) * ELL, u)] = v[i * G.R + s];
                         }
                     } else {
                         const bool g = Cfg::LAST && a.gout0 != nullptr;
