@@ -556,3 +556,68 @@ def test_single_transform_host_path_equals_device_path(oracle, prec):
         assert np.array_equal(back, G.run_c2r(rf.plan, X[None, :])[0]), order
         if prec == "f32":
             assert np.array_equal(X, oracle.rfft_forward_port(xr)), order
+
+
+@pytest.mark.parametrize("prec,ft,ct", PRECS)
+@pytest.mark.parametrize("order", [19, 20])
+def test_multipass_fast_form_two_pass_orders(oracle, prec, ft, ct, order):
+    """The fast-twiddle form at orders 19-20, which may run as two passes
+    (512 | 1024 and 1024 | 1024 points): within the tolerance of the FP64 DFT,
+    both directions, AoS and SoA, several chunks."""
+    n = 1 << order
+    rng = np.random.default_rng(3500 + order)
+    b = 3
+    x = _cx(rng, b, n, ct)
+    plan = Z.Plan(Z.C2C, order, ft, mode=Z.MODE_FAST)
+    tol = oracle.tolerance(order, prec)
+    for forward in (True, False):
+        fp64 = oracle.cfft_fp64(x, forward)
+        for il, ol in ((Z.AOS, Z.AOS), (Z.SOA, Z.SOA)):
+            y = G.run_c2c(plan, x, forward, il, ol)
+            assert oracle.rel_l2(y, fp64).max() <= tol, (order, forward, il, ol)
+
+
+def test_pass_schemes_agree_bitwise():
+    """Orders 19 and 20 in three passes (ZLFFT_PASS_SCHEME=0) and in two
+    (ZLFFT_PASS_SCHEME=1; a process each, since the switch is read once): the
+    same butterflies and twiddles, so the plain form's outputs are
+    bit-identical in both precisions, forward and backward, AoS and SoA."""
+    import os
+    import subprocess
+    import sys
+    code = r'''
+import sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+import zldsp_fft_b200 as Z
+rng = np.random.default_rng(37)
+out = {}
+for dt, ct in ((np.float32, np.complex64), (np.float64, np.complex128)):
+    for order, b in ((19, 5), (20, 3)):
+        n = 1 << order
+        x = (rng.uniform(-1, 1, (b, n)) + 1j * rng.uniform(-1, 1, (b, n))).astype(ct)
+        p = Z.Plan(Z.C2C, order, dt)
+        ti = torch.from_numpy(x.view(dt).reshape(b, n, 2).copy()).cuda()
+        f = torch.empty_like(ti); g = torch.empty_like(ti)
+        p.exec_device(Z.FORWARD, Z.AOS, Z.AOS, ti.data_ptr(), None, f.data_ptr(), None, b)
+        p.exec_device(Z.BACKWARD, Z.AOS, Z.AOS, f.data_ptr(), None, g.data_ptr(), None, b)
+        re = torch.empty(b, n, dtype=ti.dtype, device="cuda"); im = torch.empty_like(re)
+        p.exec_device(Z.FORWARD, Z.AOS, Z.SOA, ti.data_ptr(), None, re.data_ptr(), im.data_ptr(), b)
+        torch.cuda.synchronize()
+        assert p.device_status() == 0
+        k = f"{np.dtype(dt).name}_{order}"
+        out["f" + k] = f.cpu().numpy(); out["g" + k] = g.cpu().numpy()
+        out["r" + k] = re.cpu().numpy(); out["i" + k] = im.cpu().numpy()
+np.savez(sys.argv[2], **out)
+'''
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = {}
+    for flag in ("0", "1"):
+        path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"zlfft_scheme_{flag}_{os.getpid()}.npz")
+        env = dict(os.environ, ZLFFT_PASS_SCHEME=flag)
+        r = subprocess.run([sys.executable, "-c", code, root, path], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        res[flag] = dict(np.load(path))
+        os.remove(path)
+    for k in res["0"]:
+        assert np.array_equal(res["0"][k], res["1"][k]), k

@@ -152,6 +152,8 @@ struct TablesHolder {
     zlfft::TileTable f64{};
     zlfft::PassTable p32{};
     zlfft::PassTable p64{};
+    zlfft::PassTable p32s{};  // pass scheme 1, orders 19-20
+    zlfft::PassTable p64s{};
     zlfft::GatherTable g32{};
     zlfft::GatherTable g64{};
     zlfft::TcPassTable tc{};
@@ -181,6 +183,8 @@ struct TablesHolder {
         zlfft::fill_pass_f64_a(p64);
         zlfft::fill_pass_f64_b(p64);
         zlfft::fill_pass_f64_c(p64);
+        zlfft::fill_pass_split_f32(p32s);
+        zlfft::fill_pass_split_f64(p64s);
     }
 };
 
@@ -324,6 +328,7 @@ struct zlfft_plan_s {
     bool tc_form = false;   // 256-point passes in the tensor-core split form
     bool fast_form = false; // multi-pass radix-16 groups with fast twiddles (ZLFFT_MODE_FAST)
     bool fuse_split = false;  // RFFT forward: split fused into the last pass (else its own kernel)
+    int pass_scheme = 0;      // multi-pass stage grouping (zlfft_pass.cuh): 1 = two passes for orders 19-20
     int store_tma = -1;       // first pass output by TMA tensor stores (-1: the precision's default)
     // The reference's algorithm switch (src/common/zldsp_fft_common_init.hpp:305-339), where the plan
     // follows one: a CFFT order >= switch_order runs the macro path (zlfft_macro.cuh) with this micro
@@ -337,6 +342,34 @@ struct zlfft_plan_s {
 };
 
 namespace {
+
+// The multi-pass kernels of a plan's precision and pass scheme.
+const zlfft::PassTable& pass_table(const zlfft_plan_s* p) {
+    if (p->pass_scheme == 1) return p->prec == ZLFFT_F32 ? tables().p32s : tables().p64s;
+    return p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
+}
+
+// Pass scheme of a multi-pass plan: CFFT orders 19-20 may run in two passes
+// (512 | 1024 and 1024 | 1024 points) rather than three. The tensor-core form
+// keeps scheme 0 (its kernels are 256-point passes), and so does the RFFT
+// (its forward split fuses into a last pass of 128-byte unit rows).
+// Default, from same-box measurements (GB/s, three -> two passes): FP32
+// order 19 plain 1860 -> 1961, fast 2130 -> 2545; order 20 fast 2276 -> 2333
+// but plain 1913 -> 1813; FP64 slower at both orders (its 1024-point passes
+// run one CTA per SM). ZLFFT_PASS_SCHEME=0 / 1 forces three / two passes
+// wherever both exist.
+int default_pass_scheme(const zlfft_plan_s* p) {
+    static const int forced = [] {
+        const char* e = getenv("ZLFFT_PASS_SCHEME");
+        return e ? (e[0] == '0' ? 0 : 1) : -1;
+    }();
+    const bool ok = p->kind == ZLFFT_C2C && !p->tc_form && p->cfft_order >= zlfft::kPassSplitMinP &&
+                    p->cfft_order <= zlfft::kPassSplitMaxP;
+    if (!ok) return 0;
+    if (forced >= 0) return forced;
+    if (p->prec != ZLFFT_F32) return 0;
+    return (p->cfft_order == 19 || p->fast_form) ? 1 : 0;
+}
 
 struct DeviceGuard {
     int prev = -1;
@@ -565,7 +598,7 @@ zlfft::PassLaunchFn pick_pass(const zlfft_plan_s* p, int pi, bool fwd, int li, i
         if (!f) f = tt.fn[P - zlfft::kPassMinP][pi][fwd ? 1 : 0];
         if (f) return f;
     }
-    const zlfft::PassTable& t = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
+    const zlfft::PassTable& t = pass_table(p);
     if (p->fast_form && li == ZLFFT_AOS && lo == ZLFFT_AOS) {
         zlfft::PassLaunchFn f = t.fast[P - zlfft::kPassMinP][pi][fwd ? 1 : 0];
         if (f) return f;
@@ -584,7 +617,7 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
         return fail(ZLFFT_ERR_UNSUPPORTED, "order %d is above the supported maximum", p->order);
     int rc = ensure_scratch(p);
     if (rc) return rc;
-    const zlfft::PassTable& t = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
+    const zlfft::PassTable& t = pass_table(p);
     const auto& row = t.fn[P - zlfft::kPassMinP];
     int np = 0;
     while (np < zlfft::kMaxPasses && row[np][1][0][0]) ++np;
@@ -672,8 +705,7 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
             // RFFT forward: the last pass fuses the split and writes the bins
             zlfft::PassLaunchFn split_fn = nullptr;
             if (p->fuse_split && last && r2c && !p->tc_form) {
-                const zlfft::PassTable& tt = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
-                split_fn = tt.split[P - zlfft::kPassMinP][dop == zlfft::kR2CSqrMag ? 1 : 0][out_layout];
+                split_fn = pass_table(p).split[P - zlfft::kPassMinP][dop == zlfft::kR2CSqrMag ? 1 : 0][out_layout];
             }
             if ((last && !r2c) || split_fn) {
                 pa.out0 = uo0;
@@ -1152,7 +1184,7 @@ int exec_multipass_noalloc(zlfft_plan_s* p, int dop, int in_layout, int out_layo
     const long long chunk = (long long)(half / per);
     char* s0 = static_cast<char*>(base);
     char* s1 = s0 + half;
-    const zlfft::PassTable& t = p->prec == ZLFFT_F32 ? tables().p32 : tables().p64;
+    const zlfft::PassTable& t = pass_table(p);
     const auto& row = t.fn[P - zlfft::kPassMinP];
     int np = 0;
     while (np < zlfft::kMaxPasses && row[np][1][0][0]) ++np;
@@ -2031,6 +2063,7 @@ int zlfft_plan_create(zlfft_plan* out, int kind, int precision, size_t order, in
         }
         if (mode == ZLFFT_MODE_TC_FP16) p->tc_form = true;
         if (mode == ZLFFT_MODE_FAST) p->fast_form = true;
+        p->pass_scheme = default_pass_scheme(p);
     }
     cudaError_t e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {

@@ -129,9 +129,9 @@ inline PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
 // Encode the input maps of a pass: {units * comps, R, batch} with strides
 // {N/R * comps, transform stride} scalars; box {UPC * comps, RB, 1}.
 // Returns false (direct loads) when the source does not meet TMA rules.
-template <typename F, int P, int PI, int IL2>
+template <typename F, int P, int PI, int IL2, int S = 0>
 bool encode_pass_maps(const PassArgs& a, PassMaps& m) {
-    using Cfg = PassCfg<F, P, PI>;
+    using Cfg = PassCfg<F, P, PI, S>;
     if (!Cfg::kTMA) return false;
     PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
     if (!enc) return false;
@@ -157,10 +157,10 @@ bool encode_pass_maps(const PassArgs& a, PassMaps& m) {
     return true;
 }
 
-template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0, bool FAST = false>
+template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0, bool FAST = false, int S = 0>
 cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchCtx& ctx) {
-    using Cfg = PassCfg<F, P, PI>;
-    auto kern = pass_kernel<F, P, PI, FWD, IL, OL, SPLIT, FAST>;
+    using Cfg = PassCfg<F, P, PI, S>;
+    auto kern = pass_kernel<F, P, PI, FWD, IL, OL, SPLIT, FAST, S>;
     constexpr int IL2 = Cfg::FIRST ? IL : (int)kAoS;
     PassArgs a = a_in;
     PassMaps maps;
@@ -171,7 +171,7 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
         return !(e && e[0] == '0');
     }();
     // (the split-fused last pass reads mirror-paired units directly)
-    a.tma = (SPLIT == 0 && tma_enabled && a.tma && !(Cfg::FIRST && a.gin0) && encode_pass_maps<F, P, PI, IL2>(a, maps))
+    a.tma = (SPLIT == 0 && tma_enabled && a.tma && !(Cfg::FIRST && a.gin0) && encode_pass_maps<F, P, PI, IL2, S>(a, maps))
                 ? 1
                 : 0;
     // a.tma_out on entry: the plan asks for tensor stores of the first pass's output
@@ -205,9 +205,9 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
     return cudaGetLastError();
 }
 
-template <typename F, int P, int PI>
+template <typename F, int P, int PI, int S = 0>
 void fill_pass_one(PassTable& t) {
-    constexpr int np = pass_count(P);
+    constexpr int np = pass_count(P, S);
     constexpr bool first = PI == 0, last = PI + 1 == np;
     for (int f = 0; f < 2; ++f)
         for (int il = 0; il < 2; ++il)
@@ -215,19 +215,19 @@ void fill_pass_one(PassTable& t) {
     // direction only matters on the first (load swap) and last (store swap) pass
     auto& e = t.fn[P - kPassMinP][PI];
     if constexpr (first) {
-        e[1][kAoS][kAoS] = launch_pass<F, P, PI, true, kAoS, kAoS>;
-        e[1][kSoA][kAoS] = launch_pass<F, P, PI, true, kSoA, kAoS>;
-        e[0][kAoS][kAoS] = launch_pass<F, P, PI, false, kAoS, kAoS>;
-        e[0][kSoA][kAoS] = launch_pass<F, P, PI, false, kSoA, kAoS>;
+        e[1][kAoS][kAoS] = launch_pass<F, P, PI, true, kAoS, kAoS, 0, false, S>;
+        e[1][kSoA][kAoS] = launch_pass<F, P, PI, true, kSoA, kAoS, 0, false, S>;
+        e[0][kAoS][kAoS] = launch_pass<F, P, PI, false, kAoS, kAoS, 0, false, S>;
+        e[0][kSoA][kAoS] = launch_pass<F, P, PI, false, kSoA, kAoS, 0, false, S>;
         e[1][kAoS][kSoA] = e[1][kAoS][kAoS];
         e[1][kSoA][kSoA] = e[1][kSoA][kAoS];
         e[0][kAoS][kSoA] = e[0][kAoS][kAoS];
         e[0][kSoA][kSoA] = e[0][kSoA][kAoS];
     } else if constexpr (last) {
-        e[1][kAoS][kAoS] = launch_pass<F, P, PI, true, kAoS, kAoS>;
-        e[1][kAoS][kSoA] = launch_pass<F, P, PI, true, kAoS, kSoA>;
-        e[0][kAoS][kAoS] = launch_pass<F, P, PI, false, kAoS, kAoS>;
-        e[0][kAoS][kSoA] = launch_pass<F, P, PI, false, kAoS, kSoA>;
+        e[1][kAoS][kAoS] = launch_pass<F, P, PI, true, kAoS, kAoS, 0, false, S>;
+        e[1][kAoS][kSoA] = launch_pass<F, P, PI, true, kAoS, kSoA, 0, false, S>;
+        e[0][kAoS][kAoS] = launch_pass<F, P, PI, false, kAoS, kAoS, 0, false, S>;
+        e[0][kAoS][kSoA] = launch_pass<F, P, PI, false, kAoS, kSoA, 0, false, S>;
         e[1][kSoA][kAoS] = e[1][kAoS][kAoS];
         e[1][kSoA][kSoA] = e[1][kAoS][kSoA];
         e[0][kSoA][kAoS] = e[0][kAoS][kAoS];
@@ -235,36 +235,45 @@ void fill_pass_one(PassTable& t) {
     } else {
         for (int f = 0; f < 2; ++f)
             for (int il = 0; il < 2; ++il)
-                for (int ol = 0; ol < 2; ++ol) e[f][il][ol] = launch_pass<F, P, PI, true, kAoS, kAoS>;
+                for (int ol = 0; ol < 2; ++ol) e[f][il][ol] = launch_pass<F, P, PI, true, kAoS, kAoS, 0, false, S>;
     }
 }
 
-template <typename F, int P>
+template <typename F, int P, int S = 0>
 void fill_pass_order(PassTable& t) {
-    fill_pass_one<F, P, 0>(t);
-    fill_pass_one<F, P, 1>(t);
-    if constexpr (pass_count(P) > 2) fill_pass_one<F, P, 2>(t);
+    fill_pass_one<F, P, 0, S>(t);
+    fill_pass_one<F, P, 1, S>(t);
+    if constexpr (pass_count(P, S) > 2) fill_pass_one<F, P, 2, S>(t);
+    else
+        for (int f = 0; f < 2; ++f)
+            for (int il = 0; il < 2; ++il)
+                for (int ol = 0; ol < 2; ++ol) t.fn[P - kPassMinP][2][f][il][ol] = nullptr;
     // fast-twiddle form (AoS): the direction only matters on the first and last pass
-    constexpr int NP = pass_count(P);
+    constexpr int NP = pass_count(P, S);
     [&]<int... PIs>(std::integer_sequence<int, PIs...>) {
         (
             [&] {
                 auto& fe = t.fast[P - kPassMinP][PIs];
                 if constexpr (PIs == 0 || PIs + 1 == NP) {
-                    fe[1] = launch_pass<F, P, PIs, true, kAoS, kAoS, 0, true>;
-                    fe[0] = launch_pass<F, P, PIs, false, kAoS, kAoS, 0, true>;
+                    fe[1] = launch_pass<F, P, PIs, true, kAoS, kAoS, 0, true, S>;
+                    fe[0] = launch_pass<F, P, PIs, false, kAoS, kAoS, 0, true, S>;
                 } else {
-                    fe[0] = fe[1] = launch_pass<F, P, PIs, true, kAoS, kAoS, 0, true>;
+                    fe[0] = fe[1] = launch_pass<F, P, PIs, true, kAoS, kAoS, 0, true, S>;
                 }
             }(),
             ...);
     }(std::make_integer_sequence<int, NP>{});
     // last pass with the RFFT split fused: [forward | sqr_mag][output layout]
-    constexpr int PL = pass_count(P) - 1;
+    // (scheme 0: its last pass has 128-byte unit rows, which the split's mirror pairs need)
     auto& sp = t.split[P - kPassMinP];
-    sp[0][kAoS] = launch_pass<F, P, PL, true, kAoS, kAoS, kR2CFwd>;
-    sp[0][kSoA] = launch_pass<F, P, PL, true, kAoS, kSoA, kR2CFwd>;
-    sp[1][kAoS] = sp[1][kSoA] = launch_pass<F, P, PL, true, kAoS, kAoS, kR2CSqrMag>;
+    if constexpr (S == 0) {
+        constexpr int PL = pass_count(P) - 1;
+        sp[0][kAoS] = launch_pass<F, P, PL, true, kAoS, kAoS, kR2CFwd>;
+        sp[0][kSoA] = launch_pass<F, P, PL, true, kAoS, kSoA, kR2CFwd>;
+        sp[1][kAoS] = sp[1][kSoA] = launch_pass<F, P, PL, true, kAoS, kAoS, kR2CSqrMag>;
+    } else {
+        sp[0][kAoS] = sp[0][kSoA] = sp[1][kAoS] = sp[1][kSoA] = nullptr;
+    }
 }
 
 template <typename F, int... Ps>
@@ -279,6 +288,9 @@ void fill_pass_f32_c(PassTable& t);  // orders 25..26
 void fill_pass_f64_a(PassTable& t);
 void fill_pass_f64_b(PassTable& t);
 void fill_pass_f64_c(PassTable& t);
+// scheme 1 (two passes for orders 19-20), entries at the same order index
+void fill_pass_split_f32(PassTable& t);
+void fill_pass_split_f64(PassTable& t);
 
 template <typename F, int Lo, int Hi, int... Ps>
 void fill_pass_range_impl(PassTable& t, std::integer_sequence<int, Ps...>) {

@@ -31,9 +31,28 @@
 
 namespace zlfft {
 
-// Passes for order P: from the end, pairs of radix-16 groups (256 points)
-// form passes until the remaining leading groups fit 1024 points.
-__host__ __device__ constexpr int pass_count(int P) {
+// Pass schemes. Scheme 0 (every order): the tile kernel's stage groups
+// (tile_group); from the end, pairs of radix-16 groups (256 points) form
+// passes until the remaining leading groups fit 1024 points. Scheme 1 (orders
+// 19 and 20, kPassSplitMinP..kPassSplitMaxP): the third group, radix 16 at
+// sub-length L, runs as two radix-4 groups (stages L and 4L, the same
+// butterflies and twiddles, so the same arithmetic), and the passes are
+// groups [0, 3) and [3, 6): 512 | 1024 points for order 19, 1024 | 1024 for
+// order 20, two passes over the data instead of three.
+constexpr int kPassSplitMinP = 19;
+constexpr int kPassSplitMaxP = 20;
+
+__host__ __device__ constexpr int pass_num_groups(int P, int S) { return tile_num_groups(P) + (S == 1 ? 1 : 0); }
+
+__host__ __device__ constexpr Grp pass_group(int P, int S, int g) {
+    if (S == 0 || g < 2) return tile_group(P, g);
+    if (g == 2) return Grp{4, tile_group(P, 2).L, 0, 1};
+    if (g == 3) return Grp{4, 4 * tile_group(P, 2).L, 0, 1};
+    return tile_group(P, g - 1);
+}
+
+__host__ __device__ constexpr int pass_count(int P, int S = 0) {
+    if (S == 1) return 2;
     const int ng = tile_num_groups(P);
     int end = ng, n = 0;
     while (true) {
@@ -46,35 +65,38 @@ __host__ __device__ constexpr int pass_count(int P) {
 }
 
 // First group index of pass i (0-based); pass i covers groups [pass_gb(i), pass_gb(i + 1)).
-__host__ __device__ constexpr int pass_gb(int P, int i) {
-    const int ng = tile_num_groups(P);
-    const int np = pass_count(P);
+__host__ __device__ constexpr int pass_gb(int P, int i, int S = 0) {
+    const int ng = pass_num_groups(P, S);
+    const int np = pass_count(P, S);
     if (i >= np) return ng;
     if (i == 0) return 0;
+    if (S == 1) return 3;
     // passes 1..np-1 are pairs of radix-16 groups at the end
     return ng - 2 * (np - i);
 }
 
-__host__ __device__ constexpr int pass_radix(int P, int i) {
+__host__ __device__ constexpr int pass_radix(int P, int i, int S = 0) {
     int r = 1;
-    for (int g = pass_gb(P, i); g < pass_gb(P, i + 1); ++g) r *= tile_group(P, g).R;
+    for (int g = pass_gb(P, i, S); g < pass_gb(P, i + 1, S); ++g) r *= pass_group(P, S, g).R;
     return r;
 }
 
-template <typename F, int P, int PI>
+template <typename F, int P, int PI, int S = 0>
 struct PassCfg {
     using C = Cx<F>;
+    static_assert(S == 0 || (P >= kPassSplitMinP && P <= kPassSplitMaxP && tile_group(P, 2).R == 16),
+                  "pass scheme 1: orders 19-20");
     static constexpr int N = 1 << P;
-    static constexpr int GB = pass_gb(P, PI);
-    static constexpr int GE = pass_gb(P, PI + 1);
-    static constexpr int R = pass_radix(P, PI);
-    static constexpr int L_IN = tile_group(P, GB).L;
+    static constexpr int GB = pass_gb(P, PI, S);
+    static constexpr int GE = pass_gb(P, PI + 1, S);
+    static constexpr int R = pass_radix(P, PI, S);
+    static constexpr int L_IN = pass_group(P, S, GB).L;
     static constexpr int L_OUT = L_IN * R;
     static constexpr bool FIRST = (PI == 0);
-    static constexpr bool LAST = (GE == tile_num_groups(P));
+    static constexpr bool LAST = (GE == pass_num_groups(P, S));
     static constexpr int E = [] {
         int e = 1;
-        for (int g = GB; g < GE; ++g) e = tile_group(P, g).R > e ? tile_group(P, g).R : e;
+        for (int g = GB; g < GE; ++g) e = pass_group(P, S, g).R > e ? pass_group(P, S, g).R : e;
         return e;
     }();
     static constexpr int T = R / E;  // threads per unit
@@ -227,10 +249,10 @@ __device__ __forceinline__ int split_unit(int ib, int u) {
 // rfft_split_kernel does.
 //
 // FAST selects the fast-twiddle form of the radix-16 groups (group16_fast).
-template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0, bool FAST = false>
-__global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>::MINB)
+template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0, bool FAST = false, int S = 0>
+__global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, PI, S>::MINB)
     pass_kernel(const PassArgs a, const __grid_constant__ PassMaps maps) {
-    using Cfg = PassCfg<F, P, PI>;
+    using Cfg = PassCfg<F, P, PI, S>;
     using C = Cx<F>;
     constexpr int N = Cfg::N, R = Cfg::R, E = Cfg::E, T = Cfg::T, UPC = Cfg::UPC, ROW = Cfg::ROW;
     constexpr int L_IN = Cfg::L_IN, L_OUT = Cfg::L_OUT, GB = Cfg::GB, GE = Cfg::GE;
@@ -293,7 +315,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
             [&]<int... GI>(std::integer_sequence<int, GI...>) {
                 (
                     [&] {
-                        constexpr Grp G = tile_group(P, GB + GI);
+                        constexpr Grp G = pass_group(P, S, GB + GI);
                         if constexpr (G.R == 16 && !G.first) {
                             static_assert(G.R == E, "one radix-16 butterfly per thread");
                             constexpr int ELL = G.L / L_IN;
@@ -334,7 +356,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
             (
                 [&] {
                     constexpr int g = GB + GI;
-                    constexpr Grp G = tile_group(P, g);
+                    constexpr Grp G = pass_group(P, S, g);
                     constexpr int NB = E / G.R;
                     constexpr int ELL = G.L / L_IN;  // local sub-length at group entry
                     constexpr bool kLastG = (g + 1 == GE);
@@ -508,7 +530,11 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI>::THREADS, PassCfg<F, P, PI>:
         // are dead when nothing reads them after this pass: drop them from L2
         // rather than let L2 write them back to DRAM. Every thread's loaded
         // values have fed its stores of this item, so after the barrier no load
-        // of the item is outstanding.
+        // of the item is outstanding. (Rows under 128 bytes share their lines
+        // with items that other CTAs may still be reading, so those passes keep
+        // their input. Running a line's items one after another on one CTA, to
+        // drop the line after the last, measured 10% slower on the 1024-point
+        // passes: neighbouring CTAs no longer read the same lines together.)
         if constexpr (IL2 == kAoS && SPLIT == 0 && (UPC * sizeof(C)) % 128 == 0) {
             if (a.discard_in) {
                 __syncthreads();
