@@ -243,13 +243,20 @@ def host_info():
                     break
     except OSError:
         pass
+    # The reference reads these through sysconf(_SC_LEVEL{1_DCACHE,2_CACHE,3_CACHE}_SIZE); Python's
+    # os.sysconf does not know those names, so libc is asked directly (glibc's values of the three
+    # constants on Linux: 188, 191, 194).
     caches = {}
-    for key, name in (("l1d_bytes", "SC_LEVEL1_DCACHE_SIZE"), ("l2_bytes", "SC_LEVEL2_CACHE_SIZE"),
-                      ("l3_bytes", "SC_LEVEL3_CACHE_SIZE")):
-        try:
-            caches[key] = os.sysconf(name)
-        except (ValueError, OSError):
-            caches[key] = None
+    try:
+        import ctypes
+        libc = ctypes.CDLL(None)
+        libc.sysconf.restype = ctypes.c_long
+        libc.sysconf.argtypes = [ctypes.c_int]
+        for key, code in (("l1d_bytes", 188), ("l2_bytes", 191), ("l3_bytes", 194)):
+            v = int(libc.sysconf(code))
+            caches[key] = v if v >= 0 else None
+    except (OSError, AttributeError):
+        caches = {"l1d_bytes": None, "l2_bytes": None, "l3_bytes": None}
     switch = {}
     try:
         from oracle import oracle as O
