@@ -30,7 +30,8 @@ def test_noalloc_matches_exec_device_on_two_calls(oracle):
     a row so the second one runs on the scratch the first one left behind."""
     import torch
     rng = np.random.default_rng(2024)
-    for order, batch in ((16, 70), (20, 3)):  # order 16: more transforms than one scratch chunk (64)
+    # order 16: more transforms than one scratch chunk (64); order 19: its two-pass form (512 | 1024 points)
+    for order, batch in ((16, 70), (19, 5), (20, 3)):
         n = 1 << order
         plan = Z.Plan(Z.C2C, order, np.float32)
         tol = oracle.tolerance(order, "f32")
