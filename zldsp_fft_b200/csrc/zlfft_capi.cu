@@ -701,6 +701,10 @@ int exec_multipass(zlfft_plan_s* p, int dop, int in_layout, int out_layout, cons
                 const size_t eb = (pi == 0 && src_layout == ZLFFT_SOA) ? p->esize : cx;
                 pa.tma = (p->use_tma && !gfirst && aligned(src0, 16) && (!src1 || aligned(src1, 16)) &&
                           (nb == 1 || ((size_t)src_stride * eb) % 16 == 0)) ? 1 : 0;
+                if (gfirst && a.gmaps) {  // gathered: the transforms' own maps, made with the batch
+                    pa.gmaps = static_cast<const CUtensorMap*>(a.gmaps) + b0;
+                    pa.tma = p->use_tma ? 1 : 0;
+                }
             }
             // RFFT forward: the last pass fuses the split and writes the bins
             zlfft::PassLaunchFn split_fn = nullptr;
@@ -1528,6 +1532,7 @@ struct MixedGroupHost {
     int P;       // complex order
     size_t first;  // offset of the group in the gather arrays
     size_t count;
+    const void* d_maps = nullptr;  // multi-pass groups: per-transform first-pass input maps, or null
 };
 
 }  // namespace
@@ -1663,6 +1668,7 @@ zlfft::TileArgs mixed_args(const zlfft_mixed_s* m, const MixedGroupHost& g) {
     a.tma = 0;
     a.gin0 = m->d_gin + g.first;
     a.gout0 = m->d_gout + g.first;
+    a.gmaps = g.d_maps;
     return a;
 }
 
@@ -1849,6 +1855,34 @@ int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int d
             off += items[pr][cls].size() * sizeof(zlfft::MixedItem);
         }
     }
+    // Multi-pass groups: one tensor map per transform for the first pass's bulk
+    // copies (the contiguous path's single map cannot describe scattered
+    // transforms). A group with any input off 16-byte alignment keeps direct loads.
+    std::vector<CUtensorMap> h_maps;
+    std::vector<size_t> map_first(m->groups.size(), SIZE_MAX);
+    for (size_t gi = 0; gi < m->groups.size(); ++gi) {
+        const MixedGroupHost& g = m->groups[gi];
+        const zlfft_plan_s* gp = g.plan;
+        if (mixed_in_persistent(g) || g.P < zlfft::kPassMinP || tile14(gp) || gp->micro >= 0 ||
+            g.dop == zlfft::kC2RBwd)
+            continue;
+        const int* geo = pass_table(gp).first_geom[g.P - zlfft::kPassMinP];
+        if (!geo[3]) continue;
+        const size_t b = h_maps.size();
+        h_maps.resize(b + g.count);
+        bool ok = true;
+        for (size_t i = 0; i < g.count && ok; ++i)
+            ok = zlfft::encode_first_map_one(&h_maps[b + i], h_gin[g.first + i], g.prec == ZLFFT_F64, 1 << g.P,
+                                             geo[0], geo[1], geo[2]);
+        if (!ok) {
+            h_maps.resize(b);
+            continue;
+        }
+        map_first[gi] = b;
+    }
+    off = align_up(off);
+    const size_t maps_off = off;
+    off += h_maps.size() * sizeof(CUtensorMap);
     off = align_up(off);
     const size_t counter_off = off;
     off += 4 * sizeof(int);
@@ -1861,6 +1895,9 @@ int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int d
     m->d_gin = reinterpret_cast<const void**>(base + gin_off);
     m->d_gout = reinterpret_cast<void**>(base + gout_off);
     m->d_counter = reinterpret_cast<int*>(base + counter_off);
+    for (size_t gi = 0; gi < m->groups.size(); ++gi)
+        if (map_first[gi] != SIZE_MAX)
+            m->groups[gi].d_maps = base + maps_off + map_first[gi] * sizeof(CUtensorMap);
     // group records now that the gather arrays have device addresses
     {
         size_t k[2] = {0, 0};
@@ -1887,6 +1924,8 @@ int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int d
                                items[pr][cls].size() * sizeof(zlfft::MixedItem), cudaMemcpyHostToDevice);
         }
     }
+    if (e == cudaSuccess && !h_maps.empty())
+        e = cudaMemcpy(base + maps_off, h_maps.data(), h_maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(m->d_counter, 0, 4 * sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&m->cap_stream, cudaStreamNonBlocking);
     for (int i = 0; i < zlfft_mixed_s::kSideStreams && e == cudaSuccess; ++i) {

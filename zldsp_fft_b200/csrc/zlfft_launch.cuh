@@ -110,6 +110,9 @@ struct PassTable {
     PassLaunchFn split[kPassMaxP - kPassMinP + 1][2][2];
     // [order - kPassMinP][pass][fwd]: the fast-twiddle form, AoS in and out
     PassLaunchFn fast[kPassMaxP - kPassMinP + 1][kMaxPasses][2];
+    // [order - kPassMinP]: the first pass's points per unit (R), units per CTA,
+    // positions per input box and whether it stages its input (gathered maps)
+    int first_geom[kPassMaxP - kPassMinP + 1][4];
 };
 
 // cuTensorMapEncodeTiled, reached through the runtime's driver entry point
@@ -157,6 +160,23 @@ bool encode_pass_maps(const PassArgs& a, PassMaps& m) {
     return true;
 }
 
+// One transform's input map for a gathered first pass of geometry (R, UPC, RB):
+// the box of encode_pass_maps for AoS input, over a batch of one at `base`.
+inline bool encode_first_map_one(CUtensorMap* m, const void* base, bool f64, int N, int R, int UPC, int RB) {
+    PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+    if (!enc || reinterpret_cast<uintptr_t>(base) % 16 != 0) return false;
+    const size_t es = f64 ? 8 : 4;
+    const cuuint64_t row_bytes = (cuuint64_t)(N / R) * 2 * es;
+    const cuuint64_t tr_bytes = (cuuint64_t)N * 2 * es;
+    const cuuint64_t dims[3] = {(cuuint64_t)(N / R) * 2, (cuuint64_t)R, 1};
+    const cuuint64_t strides[2] = {row_bytes, tr_bytes};
+    const cuuint32_t box[3] = {(cuuint32_t)(UPC * 2), (cuuint32_t)RB, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base),
+               dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0, bool FAST = false, int S = 0>
 cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = PassCfg<F, P, PI, S>;
@@ -171,9 +191,11 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
         return !(e && e[0] == '0');
     }();
     // (the split-fused last pass reads mirror-paired units directly)
-    a.tma = (SPLIT == 0 && tma_enabled && a.tma && !(Cfg::FIRST && a.gin0) && encode_pass_maps<F, P, PI, IL2, S>(a, maps))
-                ? 1
-                : 0;
+    if (Cfg::FIRST && a.gin0) {  // gathered: per-transform maps made with the batch (PassArgs::gmaps)
+        a.tma = (SPLIT == 0 && tma_enabled && a.tma && a.gmaps && Cfg::kTMA && IL2 == kAoS) ? 1 : 0;
+    } else {
+        a.tma = (SPLIT == 0 && tma_enabled && a.tma && encode_pass_maps<F, P, PI, IL2, S>(a, maps)) ? 1 : 0;
+    }
     // a.tma_out on entry: the plan asks for tensor stores of the first pass's output
     const bool want_store = a.tma_out != 0;
     a.tma_out = 0;
@@ -241,6 +263,14 @@ void fill_pass_one(PassTable& t) {
 
 template <typename F, int P, int S = 0>
 void fill_pass_order(PassTable& t) {
+    {
+        using C0 = PassCfg<F, P, 0, S>;
+        int* g = t.first_geom[P - kPassMinP];
+        g[0] = C0::R;
+        g[1] = C0::UPC;
+        g[2] = C0::RB;
+        g[3] = C0::kTMA ? 1 : 0;
+    }
     fill_pass_one<F, P, 0, S>(t);
     fill_pass_one<F, P, 1, S>(t);
     if constexpr (pass_count(P, S) > 2) fill_pass_one<F, P, 2, S>(t);

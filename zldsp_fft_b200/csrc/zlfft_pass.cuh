@@ -168,6 +168,11 @@ struct PassArgs {
     const void* const* gin1;
     void* const* gout0;
     void* const* gout1;
+    // Gathered first pass (AoS): transform t's input tensor map is gmaps[t], in
+    // device memory (a box of the same shape as PassMaps::m0 over that one
+    // transform), so its items are prefetched by bulk copies as in the
+    // contiguous case. Null: direct loads.
+    const CUtensorMap* gmaps;
 };
 
 // Tensor maps of a pass input, encoded on the host (zlfft_launch.cuh): a 3-D
@@ -280,8 +285,15 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
     const bool use_tma = Cfg::kTMA && a.tma && SPLIT == 0;
     auto issue = [&](long long it) {  // one thread issues the item's box copies
         if (!use_tma || threadIdx.x != 0 || it >= items) return;
-        const int z = (int)(it / Cfg::CPT);
+        int z = (int)(it / Cfg::CPT);
         const int x = (int)(it % Cfg::CPT) * UPC * CMP;  // x * sizeof(F) = 16-byte multiple
+        const CUtensorMap* m0 = &maps.m0;
+        if constexpr (Cfg::FIRST && !kSoAIn) {
+            if (a.gmaps) {  // gathered: the transform's own map, batch coordinate 0
+                m0 = a.gmaps + z;
+                z = 0;
+            }
+        }
         mbar_arrive_expect_tx(bar, (uint32_t)Cfg::SBYTES);
         F* sf = reinterpret_cast<F*>(stage);
 #pragma unroll
@@ -290,7 +302,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
                 tma_load_3d(sf + (size_t)y * UPC, &maps.m0, x, y, z, bar);
                 tma_load_3d(sf + (size_t)R * UPC + (size_t)y * UPC, &maps.m1, x, y, z, bar);
             } else {
-                tma_load_3d(stage + (size_t)y * UPC, &maps.m0, x, y, z, bar);
+                tma_load_3d(stage + (size_t)y * UPC, m0, x, y, z, bar);
             }
         }
     };

@@ -127,6 +127,9 @@ struct TileArgs {
     const void* const* gin1;
     void* const* gout0;
     void* const* gout1;
+    // Gathered multi-pass transforms: one input tensor map (CUtensorMap, in
+    // device memory) per transform for the first pass's bulk copies, or null.
+    const void* gmaps;
     // RFFT forward only: window multiplied into every frame as it is loaded
     // (the STFT front end); pairs (w[2i], w[2i+1]) per complex-pair input.
     const void* win;
