@@ -1533,6 +1533,7 @@ struct MixedGroupHost {
     size_t first;  // offset of the group in the gather arrays
     size_t count;
     const void* d_maps = nullptr;  // multi-pass groups: per-transform first-pass input maps, or null
+    bool in_aligned = false;       // every input of the group is 16-byte aligned (bulk copies)
 };
 
 }  // namespace
@@ -1665,7 +1666,9 @@ zlfft::TileArgs mixed_args(const zlfft_mixed_s* m, const MixedGroupHost& g) {
     a.tws = g.plan->d_tws;
     a.rw = g.plan->d_rw;
     a.err = g.plan->d_err;
-    a.tma = 0;
+    // gathered tile launches stage their inputs by bulk copies from each pointer
+    // (the forward operations; the persistent kernel and the passes decide for themselves)
+    a.tma = (g.in_aligned && g.plan->use_tma && g.dop != zlfft::kC2RBwd) ? 1 : 0;
     a.gin0 = m->d_gin + g.first;
     a.gout0 = m->d_gout + g.first;
     a.gmaps = g.d_maps;
@@ -1682,6 +1685,7 @@ int mixed_run_group(zlfft_mixed_s* m, const MixedGroupHost& g, cudaStream_t st) 
         return exec_multipass(g.plan, g.dop, ZLFFT_AOS, ZLFFT_AOS, a, st, ctx);
     const zlfft::GatherTable& t = g.prec == ZLFFT_F32 ? tables().g32 : tables().g64;
     zlfft::TileLaunchFn fn = t.fn[g.P][g.dop];
+    if (g.plan->fast_form && t.fast[g.P][g.dop]) fn = t.fast[g.P][g.dop];  // the tuned plan's form
     if (!fn) return fail(ZLFFT_ERR_UNSUPPORTED, "no gathered kernel for order %d", g.P);
     cudaError_t e = fn(a, st, ctx);
     if (e != cudaSuccess) return cuda_fail(e, "gathered tile launch");
@@ -1860,6 +1864,10 @@ int mixed_create_impl(zlfft_mixed* out, const zlfft_desc* descs, size_t n, int d
     // transforms). A group with any input off 16-byte alignment keeps direct loads.
     std::vector<CUtensorMap> h_maps;
     std::vector<size_t> map_first(m->groups.size(), SIZE_MAX);
+    for (MixedGroupHost& g : m->groups) {
+        g.in_aligned = true;
+        for (size_t i = 0; i < g.count && g.in_aligned; ++i) g.in_aligned = aligned(h_gin[g.first + i], 16);
+    }
     for (size_t gi = 0; gi < m->groups.size(); ++gi) {
         const MixedGroupHost& g = m->groups[gi];
         const zlfft_plan_s* gp = g.plan;

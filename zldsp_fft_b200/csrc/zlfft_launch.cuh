@@ -67,12 +67,13 @@ cudaError_t launch_tile(const TileArgs& a, cudaStream_t stream, const LaunchCtx&
 // the AoS <-> AoS operations: [order][op].
 struct GatherTable {
     TileLaunchFn fn[kTileTableP + 1][5];
+    TileLaunchFn fast[kTileTableP + 1][5];  // the fast-twiddle form, orders 11 and up (not C2R)
 };
 
-template <typename F, int P, int OP>
+template <typename F, int P, int OP, bool FAST = false>
 cudaError_t launch_tile_gather(const TileArgs& a, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = TileCfg<F, P, OP>;
-    auto kern = tile_kernel<F, P, OP, kAoS, kAoS, true>;
+    auto kern = tile_kernel<F, P, OP, kAoS, kAoS, true, false, FAST>;
     static ResidentSlots slots;
     const int blocks_per_sm = resident_ctas(slots, [kern] { return occupancy_setup(kern, Cfg::THREADS, Cfg::SMEM); });
     if (a.batch <= 0) return cudaSuccess;
@@ -84,11 +85,21 @@ cudaError_t launch_tile_gather(const TileArgs& a, cudaStream_t stream, const Lau
     return cudaGetLastError();
 }
 
+template <typename F, int P>
+void fill_gather_fast(GatherTable& t) {
+    if constexpr (P >= 11) {
+        t.fast[P][kC2CFwd] = launch_tile_gather<F, P, kC2CFwd, true>;
+        t.fast[P][kC2CBwd] = launch_tile_gather<F, P, kC2CBwd, true>;
+        t.fast[P][kR2CFwd] = launch_tile_gather<F, P, kR2CFwd, true>;
+        t.fast[P][kR2CSqrMag] = launch_tile_gather<F, P, kR2CSqrMag, true>;
+    }
+}
+
 template <typename F, int... Ps>
 void fill_gather_orders(GatherTable& t, std::integer_sequence<int, Ps...>) {
     ((t.fn[Ps][kC2CFwd] = launch_tile_gather<F, Ps, kC2CFwd>, t.fn[Ps][kC2CBwd] = launch_tile_gather<F, Ps, kC2CBwd>,
       t.fn[Ps][kR2CFwd] = launch_tile_gather<F, Ps, kR2CFwd>, t.fn[Ps][kR2CSqrMag] = launch_tile_gather<F, Ps, kR2CSqrMag>,
-      t.fn[Ps][kC2RBwd] = launch_tile_gather<F, Ps, kC2RBwd>),
+      t.fn[Ps][kC2RBwd] = launch_tile_gather<F, Ps, kC2RBwd>, fill_gather_fast<F, Ps>(t)),
      ...);
 }
 void fill_gather_f32(GatherTable& t);

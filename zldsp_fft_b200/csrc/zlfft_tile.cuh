@@ -968,7 +968,9 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
     constexpr bool kSoAIn = W::kSoAIn;
     C* stage = reinterpret_cast<C*>(smem_raw) + (Cfg::kTMA1 ? 0 : (size_t)TPC * N);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::XBYTES * (Cfg::kTMA1 ? 1 : 2));
-    const bool use_tma = (Cfg::kTMA || Cfg::kTMA1) && !GATHER && a.tma;
+    // gathered transforms (AoS): one bulk copy from each transform's own pointer,
+    // where the batch found every input 16-byte aligned (a.tma)
+    const bool use_tma = (Cfg::kTMA || Cfg::kTMA1) && (!GATHER || !kSoAIn) && a.tma;
     auto issue = [&](long long t) {  // warp 0 issues the copies of tile t
         if (!use_tma || threadIdx.x >= 32 || t * TPC >= a.batch) return;
         const long long left = a.batch - t * TPC;
@@ -982,6 +984,8 @@ __global__ void __launch_bounds__(TileCfg<F, P, OP>::THREADS, TileCfg<F, P, OP>:
                 F* dst = reinterpret_cast<F*>(stage + (size_t)q * N);
                 bulk_g2s(dst, static_cast<const F*>(a.in0) + base, kSlot / 2, bar);
                 bulk_g2s(dst + N, static_cast<const F*>(a.in1) + base, kSlot / 2, bar);
+            } else if constexpr (GATHER) {
+                bulk_g2s(stage + (size_t)q * N, static_cast<const C*>(a.gin0[t * TPC + q]), kSlot, bar);
             } else {
                 bulk_g2s(stage + (size_t)q * N, static_cast<const C*>(a.in0) + base, kSlot, bar);
             }
