@@ -354,10 +354,13 @@ const zlfft::PassTable& pass_table(const zlfft_plan_s* p) {
 // keeps scheme 0 (its kernels are 256-point passes), and so does the RFFT
 // (its forward split fuses into a last pass of 128-byte unit rows).
 // Default, from same-box measurements (GB/s, three -> two passes): FP32
-// order 19 plain 1860 -> 1961, fast 2130 -> 2545; order 20 fast 2276 -> 2333
-// but plain 1913 -> 1813; FP64 slower at both orders (its 1024-point passes
-// run one CTA per SM). ZLFFT_PASS_SCHEME=0 / 1 forces three / two passes
-// wherever both exist.
+// order 19 plain 1860 -> 1961, fast 2130 -> 2545, so order 19 takes two. Order
+// 20 stays at three: fast 2276 -> 2333 is within run-to-run spread, plain
+// 1913 -> 1813 is slower, and its second 1024-point pass cannot drop the
+// intermediate from L2 (32-byte unit rows), which raises DRAM traffic from
+// 1.09x to 1.61x the algorithmic bytes. FP64 is slower at both orders (its
+// 1024-point passes run one CTA per SM). ZLFFT_PASS_SCHEME=0 / 1 forces three
+// / two passes wherever both exist.
 int default_pass_scheme(const zlfft_plan_s* p) {
     static const int forced = [] {
         const char* e = getenv("ZLFFT_PASS_SCHEME");
@@ -367,8 +370,7 @@ int default_pass_scheme(const zlfft_plan_s* p) {
                     p->cfft_order <= zlfft::kPassSplitMaxP;
     if (!ok) return 0;
     if (forced >= 0) return forced;
-    if (p->prec != ZLFFT_F32) return 0;
-    return (p->cfft_order == 19 || p->fast_form) ? 1 : 0;
+    return (p->prec == ZLFFT_F32 && p->cfft_order == 19) ? 1 : 0;
 }
 
 struct DeviceGuard {
