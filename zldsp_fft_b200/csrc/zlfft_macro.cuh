@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(DifCfg<F, G>::THREADS, 1) dif_pass_kernel(cons
 template <typename F, int M>
 struct SegCfg {
     using C = Cx<F>;
-    static constexpr int CB0 = 128 / (int)sizeof(C);
+    static constexpr int CB0 = 4;  // 32- (FP32) / 64-byte (FP64) output rows, 2 CTAs per SM
     static constexpr int CBM = (128 * 1024) / ((1 << M) * (int)sizeof(C));
     static constexpr int CB = CB0 < CBM ? CB0 : CBM;
     static constexpr int EB = tile_elems(M);
@@ -280,7 +280,7 @@ struct SegArgs {
 };
 
 template <typename F, int M, bool FWD, int OL>
-__global__ void __launch_bounds__(SegCfg<F, M>::BLOCK, 1) macro_seg_kernel(const SegArgs sa) {
+__global__ void __launch_bounds__(SegCfg<F, M>::BLOCK, SegCfg<F, M>::W::MINB) macro_seg_kernel(const SegArgs sa) {
     using SC = SegCfg<F, M>;
     using Wk = TileWorker<F, M, kC2CFwd, kAoS, kAoS, SC::BLOCK, false, false, false, true, SC::E>;
     using Cfg = typename Wk::Cfg;

@@ -549,12 +549,15 @@ struct TileWorker {
 
     __device__ __forceinline__ uint32_t sidx(int pos) const { return swz<C>(sbase + (uint32_t)pos); }
 
-    // KEEP layout: output k of slot q at k * TPC + (q ^ (k % TPC)). With TPC
-    // slots of 8-byte (FP32) or 16-byte (FP64) points filling a 128-byte row,
-    // a warp's writes of consecutive k by one slot and its reads of whole rows
-    // (all slots of consecutive k) both touch every bank once per row.
+    // KEEP layout: output k of slot q at k * TPC + (q ^ ((k / KR) % TPC)), with
+    // KR rows of TPC points per 128-byte line (1 when a row fills the line).
+    // Consecutive k of one slot (a half-warp's writes) then take distinct
+    // (row in line, slot) pairs, and whole rows (all slots of consecutive k, the
+    // transposed store's reads) are permutations within each line: both touch
+    // every bank once per line.
+    static constexpr int KR = (int)(128 / sizeof(C)) > TPC ? (int)(128 / sizeof(C)) / TPC : 1;
     static __device__ __forceinline__ uint32_t keep_idx(int k, int q) {
-        return (uint32_t)k * TPC + (uint32_t)(q ^ (k & (TPC - 1)));
+        return (uint32_t)k * TPC + (uint32_t)(q ^ ((k / KR) & (TPC - 1)));
     }
 
     // Backward RFFT: issue the cp.async copies of tile t's bins into the
