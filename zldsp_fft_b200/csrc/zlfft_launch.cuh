@@ -188,6 +188,33 @@ inline bool encode_first_map_one(CUtensorMap* m, const void* base, bool f64, int
                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Maps of the split-fused last pass (AoS scratch input): m0 boxes the item's
+// HALF low units, m1 the window of 2 HALF units that holds their mirrors.
+template <typename F, int P, int PI, int S = 0>
+bool encode_split_maps(const PassArgs& a, PassMaps& m) {
+    using Cfg = PassCfg<F, P, PI, S>;
+    if (!Cfg::kTMA_SPLIT) return false;
+    PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+    if (!enc || reinterpret_cast<uintptr_t>(a.in0) % 16 != 0) return false;
+    const CUtensorMapDataType dt = sizeof(F) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const cuuint64_t row_bytes = (cuuint64_t)(Cfg::N / Cfg::R) * 2 * sizeof(F);
+    cuuint64_t tr_bytes = (cuuint64_t)a.in_stride * 2 * sizeof(F);
+    if (a.batch == 1) tr_bytes = (cuuint64_t)Cfg::N * 2 * sizeof(F);
+    if (tr_bytes % 16 != 0 || row_bytes % 16 != 0) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)(Cfg::N / Cfg::R) * 2, (cuuint64_t)Cfg::R, (cuuint64_t)a.batch};
+    const cuuint64_t strides[2] = {row_bytes, tr_bytes};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const cuuint32_t box_lo[3] = {(cuuint32_t)(Cfg::HALF * 2), (cuuint32_t)Cfg::RB, 1};
+    const cuuint32_t box_win[3] = {(cuuint32_t)(Cfg::HALF * 4), (cuuint32_t)Cfg::RB, 1};
+    void* base = const_cast<void*>(a.in0);
+    return enc(&m.m0, dt, 3, base, dims, strides, box_lo, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+           enc(&m.m1, dt, 3, base, dims, strides, box_win, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <typename F, int P, int PI, bool FWD, int IL, int OL, int SPLIT = 0, bool FAST = false, int S = 0>
 cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchCtx& ctx) {
     using Cfg = PassCfg<F, P, PI, S>;
@@ -202,10 +229,12 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
         return !(e && e[0] == '0');
     }();
     // (the split-fused last pass reads mirror-paired units directly)
-    if (Cfg::FIRST && a.gin0) {  // gathered: per-transform maps made with the batch (PassArgs::gmaps)
-        a.tma = (SPLIT == 0 && tma_enabled && a.tma && a.gmaps && Cfg::kTMA && IL2 == kAoS) ? 1 : 0;
+    if constexpr (SPLIT != 0) {  // split-fused last pass: a low box and a mirror window per item
+        a.tma = (tma_enabled && a.tma && encode_split_maps<F, P, PI, S>(a, maps)) ? 1 : 0;
+    } else if (Cfg::FIRST && a.gin0) {  // gathered: per-transform maps made with the batch (PassArgs::gmaps)
+        a.tma = (tma_enabled && a.tma && a.gmaps && Cfg::kTMA && IL2 == kAoS) ? 1 : 0;
     } else {
-        a.tma = (SPLIT == 0 && tma_enabled && a.tma && encode_pass_maps<F, P, PI, IL2, S>(a, maps)) ? 1 : 0;
+        a.tma = (tma_enabled && a.tma && encode_pass_maps<F, P, PI, IL2, S>(a, maps)) ? 1 : 0;
     }
     // a.tma_out on entry: the plan asks for tensor stores of the first pass's output
     const bool want_store = a.tma_out != 0;
@@ -228,12 +257,13 @@ cudaError_t launch_pass(const PassArgs& a_in, cudaStream_t stream, const LaunchC
         }
     }
     static ResidentSlots slots;
-    const int blocks_per_sm = resident_ctas(slots, [kern] { return occupancy_setup(kern, Cfg::THREADS, Cfg::SMEM); });
+    constexpr size_t kSmem = SPLIT != 0 ? Cfg::SMEM_SPLIT : Cfg::SMEM;
+    const int blocks_per_sm = resident_ctas(slots, [kern] { return occupancy_setup(kern, Cfg::THREADS, kSmem); });
     if (a.batch <= 0) return cudaSuccess;
     const long long items = a.batch * Cfg::CPT;
     const long long cap = (long long)ctx.num_sms * blocks_per_sm;
     const unsigned grid = (unsigned)(items < cap ? items : cap);
-    kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(a, maps);
+    kern<<<grid, Cfg::THREADS, kSmem, stream>>>(a, maps);
     if (ctx.launches) ++*ctx.launches;
     return cudaGetLastError();
 }

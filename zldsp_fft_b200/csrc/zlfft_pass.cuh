@@ -127,6 +127,14 @@ struct PassCfg {
     // (+1024: the buffers start at the first 1024-byte boundary of the dynamic
     // shared memory, as the swizzled output boxes of the first pass require)
     static constexpr size_t SMEM = (kTMA ? SOFF + SBYTES + 16 : XBYTES) + 1024;
+    // Last pass with the RFFT split fused: the item's HALF low units (one box)
+    // and a window of 2 HALF units that holds their HALF mirrors (split_unit;
+    // a mirror block starts at an odd unit, which no bulk copy can, so the
+    // window starts at the even unit below it).
+    static constexpr int HALF = UPC / 2;
+    static constexpr size_t SBYTES_SPLIT = (size_t)3 * HALF * R * sizeof(C);
+    static constexpr bool kTMA_SPLIT = SOFF + SBYTES_SPLIT + 16 + 1024 <= 200 * 1024;
+    static constexpr size_t SMEM_SPLIT = (kTMA_SPLIT ? SOFF + SBYTES_SPLIT + 16 : XBYTES) + 1024;
     // First pass: the CTA's output block (UPC units x R contiguous points) is
     // written by tensor stores of 128-byte-swizzled boxes, 128 bytes of points
     // x UPC units each, staged in the exchange buffer.
@@ -278,13 +286,30 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
     constexpr bool kSoAIn = (IL2 == kSoA);
     constexpr int CMP = kSoAIn ? 1 : 2;  // scalars per unit in the map's innermost dimension
     C* stage = reinterpret_cast<C*>(smem + Cfg::SOFF);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + Cfg::SOFF + Cfg::SBYTES);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + Cfg::SOFF + (SPLIT != 0 ? Cfg::SBYTES_SPLIT : Cfg::SBYTES));
     const bool store_tma = Cfg::kStoreTMA && a.tma_out;
     static_assert(SPLIT == 0 || (Cfg::LAST && FWD && L_IN > 1 && Cfg::UPC >= 2 && Cfg::KROWS == 1),
                   "split fusion: RFFT forward last pass (padded layout)");
-    const bool use_tma = Cfg::kTMA && a.tma && SPLIT == 0;
+    const bool use_tma = (SPLIT == 0 ? Cfg::kTMA : Cfg::kTMA_SPLIT) && a.tma;
+    // split pass: the first unit of item ib's mirror window (item 0 holds
+    // units L_IN - 1 .. L_IN - 7 and, read directly, L_IN / 2)
+    auto split_ws = [](int ib) { return ib == 0 ? L_IN - 2 * Cfg::HALF : L_IN - Cfg::HALF * ib - Cfg::HALF; };
     auto issue = [&](long long it) {  // one thread issues the item's box copies
         if (!use_tma || threadIdx.x != 0 || it >= items) return;
+        if constexpr (SPLIT != 0) {
+            constexpr int H = Cfg::HALF;
+            const int z = (int)(it / Cfg::CPT);
+            const int ib = (int)(it % Cfg::CPT);
+            mbar_arrive_expect_tx(bar, (uint32_t)Cfg::SBYTES_SPLIT);
+            C* lo = stage;
+            C* win = stage + (size_t)H * R;
+#pragma unroll
+            for (int y = 0; y < R; y += Cfg::RB) {
+                tma_load_3d(lo + (size_t)y * H, &maps.m0, H * ib * 2, y, z, bar);
+                tma_load_3d(win + (size_t)y * 2 * H, &maps.m1, split_ws(ib) * 2, y, z, bar);
+            }
+            return;
+        }
         int z = (int)(it / Cfg::CPT);
         const int x = (int)(it % Cfg::CPT) * UPC * CMP;  // x * sizeof(F) = 16-byte multiple
         const CUtensorMap* m0 = &maps.m0;
@@ -374,7 +399,30 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
                     constexpr bool kLastG = (g + 1 == GE);
                     // ---- inputs
                     if constexpr (GI == 0) {
-                        if (use_tma) {
+                        if (use_tma && SPLIT != 0) {
+                            // low slots from the low box; mirror slots from the window
+                            // (slot H + j holds unit L_IN - (H ib + j)), except item 0's
+                            // slot H, unit L_IN / 2, read directly
+                            constexpr int H = Cfg::HALF;
+                            const C* lo = stage;
+                            const C* win = stage + (size_t)H * R;
+                            const bool direct = (ib == 0 && u == H);
+                            const int off = u < H ? u : (L_IN - (H * ib + (u - H))) - split_ws(ib);
+                            const C* src = static_cast<const C*>(a.in0) + tr * a.in_stride + U;
+#pragma unroll
+                            for (int i = 0; i < NB; ++i) {
+                                const int b = tb + i * T;
+#pragma unroll
+                                for (int rho = 0; rho < G.R; ++rho) {
+                                    const int pos = b + rho * (R / G.R);
+                                    v[i * G.R + rho] = direct ? src[(size_t)pos * (N / R)]
+                                                       : (u < H ? lo[pos * H + off] : win[pos * 2 * H + off]);
+                                }
+                            }
+                            fence_proxy_async_smem();  // reads of the staging buffer before its TMA refill
+                            __syncthreads();           // staging fully read: refill it with the next item
+                            issue(item + gridDim.x);
+                        } else if (use_tma) {
                             const F* sf = reinterpret_cast<const F*>(stage);
 #pragma unroll
                             for (int i = 0; i < NB; ++i) {
