@@ -621,9 +621,9 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
             constexpr int OLS = (SPLIT == kR2CSqrMag) ? (int)kAoS : OL;
             const CxOut<F, OLS> out(o0, o1, ob);
             F* osq = static_cast<F*>(o0) + ob;
-            for (int t = (int)threadIdx.x; t < tasks; t += Cfg::THREADS) {
+            // task t: the bin pair of slot pair (s1, s2) at positions (p1, p2)
+            auto pair_of = [&](int t, int& s1, int& p1, int& s2, int& p2) {
                 const int pos = t / HALF, us = t % HALF;
-                int s1, p1, s2, p2;  // slot and position of the pair's two values
                 if (first_item && us == 0) {
                     if (pos <= R / 2) {  // unit 0 pairs with itself
                         s1 = 0;
@@ -643,6 +643,10 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
                     s2 = us + HALF;
                     p2 = R - 1 - pos;
                 }
+            };
+            auto task = [&](int t, const C w) {
+                int s1, p1, s2, p2;
+                pair_of(t, s1, p1, s2, p2);
                 const int g1 = split_unit<L_IN, UPC>(ib, s1) + p1 * L_IN;
                 if (g1 == 0) {  // DC and Nyquist from Z[0]
                     const C z0 = sm[p1 * ROW + s1];
@@ -654,12 +658,11 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
                         osq[0] = mul_rn(dc, dc);
                         osq[N] = mul_rn(ny, ny);
                     }
-                    continue;
+                    return;
                 }
                 const C za = sm[p1 * ROW + s1], zb = sm[p2 * ROW + s2];
                 const bool low = g1 <= N / 2;  // k = min(g1, N - g1)
                 const int k = low ? g1 : N - g1;
-                const C w = rw[k];
                 const SplitOut<F> o = rfft_split<F>(low ? za : zb, low ? zb : za, w.x, w.y);
                 if constexpr (SPLIT == kR2CFwd) {
                     if (k != N / 2) out.put(k, cx<C>(o.xr_k, o.xi_k));
@@ -668,7 +671,24 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
                     if (k != N / 2) osq[k] = fma_rn(o.xr_k, o.xr_k, mul_rn(o.xi_k, o.xi_k));
                     osq[N - k] = fma_rn(o.xr_m, o.xr_m, mul_rn(o.xi_m, o.xi_m));
                 }
-            }
+            };
+            auto twiddle = [&](int t) -> C {  // the pair's split twiddle (unused for DC / Nyquist)
+                int s1, p1, s2, p2;
+                pair_of(t, s1, p1, s2, p2);
+                const int g1 = split_unit<L_IN, UPC>(ib, s1) + p1 * L_IN;
+                return g1 == 0 ? cx<C>((F)0, (F)0) : rw[g1 <= N / 2 ? g1 : N - g1];
+            };
+            // The HALF * R regular tasks, NT per thread: every twiddle is loaded
+            // before the first is used (looped one task at a time, each task's
+            // L2 round trip stalled the CTA: 8 per item).
+            constexpr int NT = HALF * R / Cfg::THREADS;
+            static_assert(HALF * R % Cfg::THREADS == 0, "split tasks: whole rounds of the CTA");
+            C wv[NT];
+#pragma unroll
+            for (int j = 0; j < NT; ++j) wv[j] = twiddle((int)threadIdx.x + j * Cfg::THREADS);
+#pragma unroll
+            for (int j = 0; j < NT; ++j) task((int)threadIdx.x + j * Cfg::THREADS, wv[j]);
+            if (tasks > HALF * R && threadIdx.x == 0) task(HALF * R, twiddle(HALF * R));  // item 0's last pair
         }
         // shared memory is rewritten by the next item's first exchange only after a barrier
     }
