@@ -189,7 +189,7 @@ inline bool encode_first_map_one(CUtensorMap* m, const void* base, bool f64, int
 }
 
 // Maps of the split-fused last pass (AoS scratch input): m0 boxes the item's
-// HALF low units, m1 the window of 2 HALF units that holds their mirrors.
+// HALF low units, m1 the window of HALF + 2 units that holds their mirrors.
 template <typename F, int P, int PI, int S = 0>
 bool encode_split_maps(const PassArgs& a, PassMaps& m) {
     using Cfg = PassCfg<F, P, PI, S>;
@@ -205,7 +205,7 @@ bool encode_split_maps(const PassArgs& a, PassMaps& m) {
     const cuuint64_t strides[2] = {row_bytes, tr_bytes};
     const cuuint32_t estr[3] = {1, 1, 1};
     const cuuint32_t box_lo[3] = {(cuuint32_t)(Cfg::HALF * 2), (cuuint32_t)Cfg::RB, 1};
-    const cuuint32_t box_win[3] = {(cuuint32_t)(Cfg::HALF * 4), (cuuint32_t)Cfg::RB, 1};
+    const cuuint32_t box_win[3] = {(cuuint32_t)(Cfg::WIN * 2), (cuuint32_t)Cfg::RB, 1};
     void* base = const_cast<void*>(a.in0);
     return enc(&m.m0, dt, 3, base, dims, strides, box_lo, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,

@@ -128,11 +128,13 @@ struct PassCfg {
     // shared memory, as the swizzled output boxes of the first pass require)
     static constexpr size_t SMEM = (kTMA ? SOFF + SBYTES + 16 : XBYTES) + 1024;
     // Last pass with the RFFT split fused: the item's HALF low units (one box)
-    // and a window of 2 HALF units that holds their HALF mirrors (split_unit;
-    // a mirror block starts at an odd unit, which no bulk copy can, so the
-    // window starts at the even unit below it).
+    // and a window of WIN = HALF + 2 units that holds their HALF mirrors
+    // (split_unit; a mirror block starts at an odd unit, which no bulk copy
+    // can, so the window starts at the even unit below it). With the 2 HALF
+    // window of the first version the pass held two CTAs per SM instead of three.
     static constexpr int HALF = UPC / 2;
-    static constexpr size_t SBYTES_SPLIT = (size_t)3 * HALF * R * sizeof(C);
+    static constexpr int WIN = HALF + 2;
+    static constexpr size_t SBYTES_SPLIT = (size_t)(HALF + WIN) * R * sizeof(C);
     static constexpr bool kTMA_SPLIT = SOFF + SBYTES_SPLIT + 16 + 1024 <= 200 * 1024;
     static constexpr size_t SMEM_SPLIT = (kTMA_SPLIT ? SOFF + SBYTES_SPLIT + 16 : XBYTES) + 1024;
     // First pass: the CTA's output block (UPC units x R contiguous points) is
@@ -293,7 +295,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
     const bool use_tma = (SPLIT == 0 ? Cfg::kTMA : Cfg::kTMA_SPLIT) && a.tma;
     // split pass: the first unit of item ib's mirror window (item 0 holds
     // units L_IN - 1 .. L_IN - 7 and, read directly, L_IN / 2)
-    auto split_ws = [](int ib) { return ib == 0 ? L_IN - 2 * Cfg::HALF : L_IN - Cfg::HALF * ib - Cfg::HALF; };
+    auto split_ws = [](int ib) { return ib == 0 ? L_IN - Cfg::WIN : L_IN - Cfg::HALF * ib - Cfg::HALF; };
     auto issue = [&](long long it) {  // one thread issues the item's box copies
         if (!use_tma || threadIdx.x != 0 || it >= items) return;
         if constexpr (SPLIT != 0) {
@@ -306,7 +308,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
 #pragma unroll
             for (int y = 0; y < R; y += Cfg::RB) {
                 tma_load_3d(lo + (size_t)y * H, &maps.m0, H * ib * 2, y, z, bar);
-                tma_load_3d(win + (size_t)y * 2 * H, &maps.m1, split_ws(ib) * 2, y, z, bar);
+                tma_load_3d(win + (size_t)y * Cfg::WIN, &maps.m1, split_ws(ib) * 2, y, z, bar);
             }
             return;
         }
@@ -416,7 +418,7 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
                                 for (int rho = 0; rho < G.R; ++rho) {
                                     const int pos = b + rho * (R / G.R);
                                     v[i * G.R + rho] = direct ? src[(size_t)pos * (N / R)]
-                                                       : (u < H ? lo[pos * H + off] : win[pos * 2 * H + off]);
+                                                       : (u < H ? lo[pos * H + off] : win[pos * Cfg::WIN + off]);
                                 }
                             }
                             fence_proxy_async_smem();  // reads of the staging buffer before its TMA refill
