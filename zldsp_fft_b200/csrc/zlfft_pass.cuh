@@ -227,7 +227,7 @@ __host__ __device__ constexpr int digit_fold(int x) {
 //   pass of CFFT<float> order 18, 40% of its shared-memory wavefronts were
 //   conflicts.
 template <class Cfg>
-__device__ __forceinline__ int pass_xidx(int pt, int pc, int u) {
+__host__ __device__ __forceinline__ int pass_xidx(int pt, int pc, int u) {
     if constexpr (Cfg::KROWS == 1) {
         return (pt + pc) * Cfg::ROW + u;
     } else {
