@@ -1,5 +1,7 @@
-// Host-side check of the multi-pass kernel's exchange layout (pass_xidx in
-// zlfft_pass.cuh), compiled by nvcc and run on the CPU: no GPU is involved.
+// Host-side check of two shared-memory layouts, compiled by nvcc and run on
+// the CPU (no GPU is involved): the multi-pass kernel's exchange (pass_xidx in
+// zlfft_pass.cuh), and the macro path's segment tiles (TileWorker::keep_idx in
+// zlfft_tile.cuh, the columns kept for the transposed store).
 //
 // For every pass whose unit rows are shorter than a 128-byte line (the 512-
 // and 1024-point passes, XOR-swizzled layout), it replays the positions each
@@ -16,6 +18,7 @@
 #include <set>
 #include <vector>
 
+#include "zlfft_macro.cuh"
 #include "zlfft_pass.cuh"
 
 using namespace zlfft;
@@ -23,6 +26,7 @@ using namespace zlfft;
 namespace {
 
 int g_fail = 0;
+bool g_quiet = false;  // the control run: its failures are expected, not printed
 
 // Wavefronts above one per phase: phase lanes that share a bank group but not an address.
 template <class Cfg>
@@ -52,7 +56,7 @@ void access(const char* what, int w, PosFn pt_pc, UnitFn unit, int& total) {
         idx.push_back(pass_xidx<Cfg>(pt, pc, unit(t)));
     }
     const int c = conflicts<Cfg>(idx);
-    if (c && total == 0) std::printf("  first conflict: %s, warp %d, %d extra wavefronts\n", what, w, c);
+    if (c && total == 0 && !g_quiet) std::printf("  first conflict: %s, warp %d, %d extra wavefronts\n", what, w, c);
     total += c;
 }
 
@@ -69,14 +73,14 @@ int replay(int* bad_out) {
             const int i = pass_xidx<Cfg>(pos, 0, u);
             if (i < 0 || i >= R * UPC || !seen.insert(i).second) ++bad;
         }
-    if (bad) std::printf("  %d slots out of range or taken twice\n", bad);
+    if (bad && !g_quiet) std::printf("  %d slots out of range or taken twice\n", bad);
     // a split into disjoint parts gives the position's own index
     for (int pt = 0; pt < R; ++pt)
         for (int pc = 0; pc < R; pc += 1)
             if ((pt & pc) == 0 && pt + pc < R)
                 for (int u = 0; u < UPC; ++u)
                     if (pass_xidx<Cfg>(pt, pc, u) != pass_xidx<Cfg>(pt + pc, 0, u)) ++bad;
-    if (bad) std::printf("  a disjoint split changes the index\n");
+    if (bad && !g_quiet) std::printf("  a disjoint split changes the index\n");
     int total = 0;
     auto unit = [](int t) { return t % UPC; };
     for (int g = Cfg::GB; g < Cfg::GE; ++g) {
@@ -137,6 +141,56 @@ struct Padded18 : PassCfg<float, 18, 0, 0> {
 
 }  // namespace
 
+// Segment tiles of the macro path at micro order M: TPC columns of N points,
+// point k of column q at keep_idx(k, q). Writes: the last stage group writes
+// consecutive points of one column per thread group; reads: the transposed
+// store reads consecutive elements k * TPC + q.
+template <typename F, int M>
+void check_keep(const char* name) {
+    using SC = SegCfg<F, M>;
+    using Wk = TileWorker<F, M, kC2CFwd, kAoS, kAoS, SC::BLOCK, false, false, false, true, SC::E>;
+    using C = Cx<F>;
+    constexpr int N = 1 << M, TPC = Wk::TPC, T = Wk::T, BLOCK = SC::BLOCK;
+    constexpr int SL = 128 / (int)sizeof(C), lanes = SL;  // bank groups per line, lanes per phase
+    int bad = 0, extra = 0;
+    std::set<int> seen;
+    for (int k = 0; k < N; ++k)
+        for (int q = 0; q < TPC; ++q) {
+            const int i = (int)Wk::keep_idx(k, q);
+            if (i < 0 || i >= TPC * N || !seen.insert(i).second) ++bad;
+        }
+    auto phase_extra = [&](const std::vector<int>& idx) {
+        for (size_t ph = 0; ph < idx.size(); ph += lanes) {
+            std::map<int, std::set<int>> bank;
+            for (size_t l = ph; l < ph + lanes && l < idx.size(); ++l) bank[idx[l] % SL].insert(idx[l]);
+            int worst = 1;
+            for (auto& kv : bank) worst = (int)kv.second.size() > worst ? (int)kv.second.size() : worst;
+            extra += worst - 1;
+        }
+    };
+    for (int w = 0; w < BLOCK / 32; ++w) {
+        for (int off = 0; off < N; off += T) {  // writes: thread t holds point (t % T) + off of column t / T
+            std::vector<int> idx;
+            for (int lane = 0; lane < 32; ++lane) {
+                const int t = 32 * w + lane;
+                idx.push_back((int)Wk::keep_idx(t % T + off, t / T));
+            }
+            phase_extra(idx);
+        }
+        for (int e0 = 0; e0 < TPC * N; e0 += BLOCK) {  // reads: element e = k * TPC + q
+            std::vector<int> idx;
+            for (int lane = 0; lane < 32; ++lane) {
+                const int e = e0 + 32 * w + lane;
+                idx.push_back((int)Wk::keep_idx(e / TPC, e % TPC));
+            }
+            phase_extra(idx);
+        }
+    }
+    std::printf("%-34s %2d columns of %5d points: %s (%d extra wavefronts)\n", name, TPC, N,
+                (bad || extra) ? "FAIL" : "ok", extra);
+    if (bad || extra) ++g_fail;
+}
+
 int main() {
     check<float, 17, 0, 0>("CFFT<float> order 17 pass 0");
     check<float, 18, 0, 0>("CFFT<float> order 18 pass 0");
@@ -151,7 +205,18 @@ int main() {
     check<double, 20, 0, 1>("CFFT<double> order 20 pass 0 (two)");
     check<double, 20, 1, 1>("CFFT<double> order 20 pass 1 (two)");
     check<double, 26, 0, 0>("CFFT<double> order 26 pass 0");
+    check_keep<float, 8>("segment tiles, float, micro 8");
+    check_keep<float, 9>("segment tiles, float, micro 9");
+    check_keep<float, 10>("segment tiles, float, micro 10");
+    check_keep<float, 11>("segment tiles, float, micro 11");
+    check_keep<float, 12>("segment tiles, float, micro 12");
+    check_keep<double, 8>("segment tiles, double, micro 8");
+    check_keep<double, 9>("segment tiles, double, micro 9");
+    check_keep<double, 10>("segment tiles, double, micro 10");
+    check_keep<double, 11>("segment tiles, double, micro 11");
+    check_keep<double, 12>("segment tiles, double, micro 12");
     int bad = 0;
+    g_quiet = true;
     const int padded = replay<Padded18, 18, 0>(&bad);
     std::printf("control: padded rows on CFFT<float> order 18 pass 0: %d extra wavefronts (%s)\n", padded,
                 padded > 0 ? "detected" : "NOT DETECTED");

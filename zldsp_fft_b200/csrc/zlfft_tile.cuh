@@ -556,7 +556,7 @@ struct TileWorker {
     // transposed store's reads) are permutations within each line: both touch
     // every bank once per line.
     static constexpr int KR = (int)(128 / sizeof(C)) > TPC ? (int)(128 / sizeof(C)) / TPC : 1;
-    static __device__ __forceinline__ uint32_t keep_idx(int k, int q) {
+    static __host__ __device__ __forceinline__ uint32_t keep_idx(int k, int q) {
         return (uint32_t)k * TPC + (uint32_t)(q ^ ((k / KR) & (TPC - 1)));
     }
 
