@@ -376,7 +376,7 @@ def test_repeated_runs_identical(oracle, case):
 
 @pytest.mark.parametrize("case", ["c2c_f32_order16", "r2c_f32_order17", "c2r_f32_order17", "c2c_f64_order15"])
 def test_host_batched_multichunk_equals_device(case):
-    """zlfft_exec_host_batched over several 32 MiB staging chunks of a
+    """zlfft_exec_host_batched over several staging chunks of a
     multi-pass order (the chunks alternate between two streams and share the
     plan's scratch), from pageable and from pinned host buffers, run three
     times: bit-identical to the device-pointer path on the same input."""

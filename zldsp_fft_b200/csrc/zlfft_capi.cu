@@ -1455,17 +1455,23 @@ int exec_host_impl(zlfft_plan_s* p, int op, int in_layout, int out_layout, const
         for (int q = 0; q < in_parts; ++q)
             memcpy(static_cast<char*>(p->h_in) + q * in_part * batch, src[q], in_part * batch);
     }
-    // Chunking: about 32 MiB of input per chunk, at least one transform
-    // (ZLFFT_HOST_CHUNK_MB overrides). Measured on the 2 GiB CFFT<float>
-    // orders 14/16/20, forward + backward from pinned buffers: 16 MiB 87.9-88.5
-    // GB/s, 32 MiB 92.1, 64 MiB 90.6 (three streams: no better).
-    static const size_t chunk_mb = [] {
+    // Chunking: an eighth of the call's input, within 8-32 MiB, at least one
+    // transform (ZLFFT_HOST_CHUNK_MB fixes the size). Measured from pinned
+    // buffers: the 2 GiB CFFT<float> orders 14/16/20, forward + backward, 16 MiB
+    // 87.9-88.5 GB/s, 32 MiB 92.1, 64 MiB 90.6 (three streams: no better);
+    // CFFT<double> order 16 x 512 (512 MiB) 88.1 -> 89.7 from 16 to 32 MiB; but
+    // RFFT<float> order 12 x 8192 (128 MiB) 79.1 -> 76.8, where fewer chunks
+    // leave more of the first copy in and the last copy out unoverlapped.
+    static const size_t chunk_env = [] {
         const char* e = getenv("ZLFFT_HOST_CHUNK_MB");
         const long v = e ? atol(e) : 0;
-        return v > 0 ? (size_t)v : (size_t)32;
+        return v > 0 ? (size_t)v << 20 : (size_t)0;
     }();
+    const size_t in_total = in_part * in_parts * batch;
+    const size_t chunk_bytes =
+        chunk_env ? chunk_env : std::min<size_t>(std::max<size_t>(in_total / 8, size_t{8} << 20), size_t{32} << 20);
     constexpr int nss = 2;
-    size_t chunk = (chunk_mb << 20) / (in_part * in_parts);
+    size_t chunk = chunk_bytes / (in_part * in_parts);
     if (chunk == 0) chunk = 1;
     if (chunk > batch) chunk = batch;
     // The chunks' copies alternate between two streams. Their transforms share
