@@ -293,8 +293,9 @@ __global__ void __launch_bounds__(PassCfg<F, P, PI, S>::THREADS, PassCfg<F, P, P
     static_assert(SPLIT == 0 || (Cfg::LAST && FWD && L_IN > 1 && Cfg::UPC >= 2 && Cfg::KROWS == 1),
                   "split fusion: RFFT forward last pass (padded layout)");
     const bool use_tma = (SPLIT == 0 ? Cfg::kTMA : Cfg::kTMA_SPLIT) && a.tma;
-    // split pass: the first unit of item ib's mirror window (item 0 holds
-    // units L_IN - 1 .. L_IN - 7 and, read directly, L_IN / 2)
+    // split pass: the first unit of item ib's mirror window (item 0's window is
+    // the last WIN units, which hold its mirrors L_IN - 1 .. L_IN - (HALF - 1);
+    // its remaining slot, unit L_IN / 2, is read directly)
     auto split_ws = [](int ib) { return ib == 0 ? L_IN - Cfg::WIN : L_IN - Cfg::HALF * ib - Cfg::HALF; };
     auto issue = [&](long long it) {  // one thread issues the item's box copies
         if (!use_tma || threadIdx.x != 0 || it >= items) return;
